@@ -1,0 +1,194 @@
+/*
+ * tups_b200 — B200 (sm_100a) implementation of the TUPS parquet loop hot path.
+ *
+ * C ABI: plain pointers, sizes and int status codes; no C++ or torch types.
+ * Every complex array crossing this boundary is complex(dp) / double _Complex,
+ * i.e. interleaved (re, im) doubles, passed as `double*` with 2*n entries, in
+ * the reference's Fortran column-major layout, so a Fortran caller hands over
+ * `c_loc(array)` without transposes.
+ *
+ * The reference keeps all state in module globals (SRC/parquet_ini.f90:67-285)
+ * and its entry points take at most an iteration counter.  Here that state
+ * lives on the GPU inside an opaque context; each entry point below replaces
+ * the Fortran routine cited beside it and operates on the context's
+ * device-resident state.  Host copies move only through tups_get_* /
+ * tups_set_*.
+ *
+ * Threading: one context per process and thread; not re-entrant.
+ * Status: 0 = ok, negative = error (TUPS_ERR_*); tups_last_error() gives
+ * the message.  Nothing here aborts the process.
+ */
+#ifndef TUPS_B200_H
+#define TUPS_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TUPS_OK 0
+#define TUPS_ERR_CUDA (-1)      /* a CUDA runtime call failed */
+#define TUPS_ERR_OOM (-2)       /* device allocation failed */
+#define TUPS_ERR_MU_NOCONV (-3) /* mu bisection exceeded its step cap */
+#define TUPS_ERR_NAN (-4)       /* NaN/Inf in Sigma or a vertex */
+#define TUPS_ERR_TIMEOUT (-5)   /* a bounded device wait ran out */
+#define TUPS_ERR_BADDIM (-6)    /* unsupported or inconsistent sizes */
+#define TUPS_ERR_BADARG (-7)    /* bad argument (NULL pointer, index range) */
+#define TUPS_ERR_IO (-8)        /* input file unreadable or malformed */
+#define TUPS_ERR_STATE (-9)     /* call order violated (e.g. PAE before PhiR) */
+
+/* channel numbering as in the reference's select case(channel): d, m, s, t */
+#define TUPS_CH_D 0
+#define TUPS_CH_M 1
+#define TUPS_CH_S 2
+#define TUPS_CH_T 3
+
+/* Input parameters: the 21-record prms file (SRC/parquet_ini.f90:300-322)
+ * plus the extensions that the reference hard-codes (t', SRC/parquet_ini.f90:24)
+ * or does not have (absolute convergence norm). */
+typedef struct tups_params {
+  double beta;          /* prms record 1 */
+  double U;             /* 2 */
+  double nParticle;     /* 3 */
+  int Nx;               /* 4 (Ny = Nx) */
+  int Nf;               /* 5, even */
+  int neighbours;       /* 6 */
+  int readinpick;       /* 7 */
+  char pick_file[256];  /* 8 */
+  int Ngrain;           /* 9 */
+  int f_range;          /* 10 */
+  double f_damping;     /* 11 */
+  int ite_max;          /* 12 */
+  int DGA;              /* 13 (must be 0: the DGA input path is not on the hot path) */
+  char fname_L[256];    /* 14 */
+  int use_sig_dmft;     /* 15 */
+  char fname_sig_dmft[256]; /* 16 */
+  int use_U2;           /* 17 */
+  int save_F;           /* 18 */
+  int oneshot;          /* 19 */
+  int old;              /* 20 (must be 0) */
+  int SDE_old;          /* 21 (must be 0) */
+  double tprime;        /* extension: -4 t' cos kx cos ky in the dispersion */
+  double conv_abs;      /* extension: converged when max|dSigma| < conv_abs (0 = reference test) */
+} tups_params;
+
+/* Derived sizes (SRC/parquet_ini.f90:326-349, SRC/preprocessing.f90:127-133). */
+typedef struct tups_dims {
+  int Nx, Ny, Nf, Ngrain;
+  int Nx_IBZ, NIBZ, Nred, Nc;
+  int Nl, Nz, Nt, Nb, NR;
+  int nbox;      /* (2*f_range+1)*Nf */
+  int wperTask;  /* Nf/2 at one task */
+} tups_dims;
+
+/* Output of conv() (SRC/parquet_check.f90:39-150) */
+typedef struct tups_conv_info {
+  double rel_sig_max;   /* max |SigmaOld-Sigma|/|Sigma| */
+  double rel_sig_av;    /* |sum(...)|/Nt */
+  double dsigma_inf;    /* max |SigmaOld-Sigma| (extension norm) */
+  double F_max[4];      /* max |F_r| */
+  double rel_err[4];    /* |1 - max|F_r| / previous max|F_r|| */
+  double mu;
+  int bisection_steps;
+  int converged;
+} tups_conv_info;
+
+typedef struct tups_ctx tups_ctx;
+
+/* ---- setup ------------------------------------------------------------ */
+/* set_parameters: parse the 21-record prms file (SRC/parquet_ini.f90:289-324).
+ * t' and conv_abs are set to 0. */
+int tups_read_prms(const char* path, tups_params* out);
+/* Initialization + FF_array + do_preprocessing's vertex init
+ * (SRC/parquet_util.f90:14-478, SRC/parquet_formfactors.f90:11-90,
+ * SRC/preprocessing.f90:100-133): builds all tables on the host, allocates and
+ * fills device state on `device`. */
+int tups_ctx_create(const tups_params* p, int device, tups_ctx** out);
+int tups_ctx_destroy(tups_ctx* ctx);
+int tups_get_dims(const tups_ctx* ctx, tups_dims* out);
+const char* tups_last_error(const tups_ctx* ctx);
+const char* tups_strerror(int status);
+
+/* ---- module parquet_chi ---------------------------------------------- */
+/* calc_Gkw_Grt(ite, Grt, cal_chi) (SRC/parquet_chi.f90:18-210): Sigma_H, mu
+ * bisection (capped; TUPS_ERR_MU_NOCONV), G(r,tau) and G(k,nu).  The chi0
+ * readout branch (:216-430) is not part of this call. */
+int tups_calc_Gkw_Grt(tups_ctx* ctx, int ite, int cal_chi);
+/* calc_chi(map_q, chi_ph_LL, chi_pp_LL) (SRC/parquet_chi.f90:438-523) for the
+ * 1-based bosonic IBZ slot idx_q; writes the dense (Nz,Nz) matrices to host. */
+int tups_calc_chi(tups_ctx* ctx, int idx_q, double* chi_ph_LL, double* chi_pp_LL);
+
+/* ---- module Parquet_kernel ------------------------------------------- */
+/* BSE(ite) (SRC/parquet_BSE.f90:19-135): on exit G_r holds Phi_r. */
+int tups_BSE(tups_ctx* ctx, int ite);
+
+/* ---- module parquet_PhiR --------------------------------------------- */
+int tups_calculate_expSqR(tups_ctx* ctx);  /* SRC/parquet_PhiR.f90:360-395 */
+int tups_calculate_expqSR(tups_ctx* ctx);  /* SRC/parquet_PhiR.f90:400-435 */
+int tups_calc_PhiR(tups_ctx* ctx, int ite); /* SRC/parquet_PhiR.f90:35-109 */
+
+/* ---- module parquet_EQMatrix (iteration 0) -------------------------- */
+int tups_calc_M_phbar_to_ph(tups_ctx* ctx); /* SRC/parquet_EQMatrix.f90:21-123 */
+int tups_calc_M_pp_to_ph(tups_ctx* ctx);    /* SRC/parquet_EQMatrix.f90:126-194 */
+int tups_calc_M_ph_to_pp(tups_ctx* ctx);    /* SRC/parquet_EQMatrix.f90:198-271 */
+int tups_calc_M_phbar_to_pp(tups_ctx* ctx); /* SRC/parquet_EQMatrix.f90:274-360 */
+
+/* ---- module parquet_EQOuter / parquet_EQContribs -------------------- */
+/* calculate_PAE (SRC/parquet_EQOuter.f90:16-118) with all crossing
+ * contributions of SRC/parquet_EQContribs.f90:44-524; F_r is written once. */
+int tups_calculate_PAE(tups_ctx* ctx);
+
+/* ---- module parquet_SDE ---------------------------------------------- */
+/* calc_SDE(ite, Grt) (SRC/parquet_SDE.f90:27-258); saves SigmaOld first,
+ * as loop.f90:152 does. */
+int tups_calc_SDE(tups_ctx* ctx, int ite);
+
+/* ---- module parquet_check -------------------------------------------- */
+/* conv() (SRC/parquet_check.f90:39-150); also SigmaOld = Sigma. */
+int tups_conv(tups_ctx* ctx, tups_conv_info* info);
+
+/* ---- loop.f90 --------------------------------------------------------- */
+/* Gamma_r = F_r - Phi_r (SRC/loop.f90:219-222) */
+int tups_vertex_update(tups_ctx* ctx);
+/* the every-5-iterations readout's effect on the trajectory (SRC/loop.f90:195,
+ * SRC/parquet_chi.f90:114-122): mu <- midpoint of [mu-U, mu+U] */
+int tups_output_block(tups_ctx* ctx);
+/* one pass of execute_loop (SRC/loop.f90:51-244) without HDF5 output */
+int tups_iteration(tups_ctx* ctx, int ite, tups_conv_info* info);
+/* execute_loop (SRC/loop.f90:29-249); *ite_out = iterations done */
+int tups_execute_loop(tups_ctx* ctx, int* ite_out, int* converged);
+
+/* ---- state in/out (host buffers, reference layouts) ------------------ */
+int tups_get_sigma(tups_ctx* ctx, double* sigma);         /* (Nt) */
+int tups_set_sigma(tups_ctx* ctx, const double* sigma);   /* (Nt) */
+int tups_get_sigma_old(tups_ctx* ctx, double* sigma);     /* (Nt) */
+int tups_get_Gkw(tups_ctx* ctx, double* gkw);             /* (Nt) */
+int tups_get_Grt(tups_ctx* ctx, double* grt);             /* (Nx*Ng, Ny*Ng, Nf) */
+int tups_get_mu(tups_ctx* ctx, double* mu);
+int tups_set_mu(tups_ctx* ctx, double mu);
+/* which: 0 = F_r (complete vertex), 1 = G_r (Gamma_r, or Phi_r between BSE
+ * and the vertex update); layout (Nz, Nz, Nb) */
+int tups_get_vertex(tups_ctx* ctx, int channel, int which, double* host);
+int tups_set_vertex(tups_ctx* ctx, int channel, int which, const double* host);
+int tups_get_PhiR(tups_ctx* ctx, int channel, double* host);  /* (Nz*Nz, Nf/2, NR) */
+/* which: 0 phbar_to_ph, 1 pp_to_ph, 2 ph_to_pp, 3 phbar_to_pp;
+ * layout (Nl, Nl, Nl, Nl, Nb, NR) as M_* of SRC/parquet_EQMatrix.f90:12-16 */
+int tups_get_M(tups_ctx* ctx, int which, double* host);
+int tups_get_expSqR(tups_ctx* ctx, double* host);   /* (NIBZ, NR, 8) */
+int tups_get_expqSR(tups_ctx* ctx, double* host);   /* (Nc, NR, 8) */
+/* form-factor tables: FF (Nx,Ny,Nl) and FF_inv (8,Nx,Ny,Nl) real; signs,
+ * reps (Nl); l-space symmetry maps lsym (8,Nl) 1-based, lfac (8,Nl);
+ * index_bosonic_IBZ (3,Nred) 1-based. Any pointer may be NULL. */
+int tups_get_tables(tups_ctx* ctx, double* FF, double* FF_inv, int* signs, int* reps,
+                    int* lsym, double* lfac, int* ibz);
+/* SDE intermediates of the last calc_SDE: chi_aux_ph/pp (Nl*nbox, Nb) and
+ * LChi, PhChi, PPChi (Nz, Nb); any pointer may be NULL */
+int tups_get_sde_aux(tups_ctx* ctx, double* chi_aux_ph, double* chi_aux_pp,
+                     double* LChi, double* PhChi, double* PPChi);
+int tups_synchronize(tups_ctx* ctx);
+/* number of this library's kernels launched since context creation */
+long long tups_kernel_launches(const tups_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TUPS_B200_H */

@@ -1,0 +1,358 @@
+// C-ABI entry points: one per Fortran routine of the hot path, operating on
+// the device-resident state of a context, plus the loop of SRC/loop.f90.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "tups_internal.h"
+
+using tups::cplx;
+
+#define TRY(x)                      \
+  do {                              \
+    int _rc = (x);                  \
+    if (_rc != TUPS_OK) return _rc; \
+  } while (0)
+
+namespace {
+
+constexpr int kMuMaxSteps = 200;  // the reference's bisection has no cap
+
+int set_dev(tups_ctx* ctx) { return tups::cuda_check(ctx, cudaSetDevice(ctx->device), "cudaSetDevice"); }
+
+int read_scalars(tups_ctx* ctx, double* out) {
+  TRY(tups::cuda_check(ctx,
+                       cudaMemcpyAsync(out, ctx->s.scal, tups::S_COUNT * sizeof(double), cudaMemcpyDeviceToHost,
+                                       ctx->stream),
+                       "read scalars"));
+  return tups::cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "synchronize");
+}
+
+// surface a status left by a device routine (bisection cap) and clear it
+int device_status(tups_ctx* ctx) {
+  double sc[tups::S_COUNT];
+  TRY(read_scalars(ctx, sc));
+  int st = (int)sc[tups::S_STATUS];
+  if (st != 0) {
+    double z = 0.0;
+    cudaMemcpy(ctx->s.scal + tups::S_STATUS, &z, sizeof(double), cudaMemcpyHostToDevice);
+    if (st == TUPS_ERR_MU_NOCONV)
+      return tups::set_error(ctx, st, "mu bisection exceeded " + std::to_string(kMuMaxSteps) + " steps");
+    return tups::set_error(ctx, st, "device routine reported an error");
+  }
+  return TUPS_OK;
+}
+
+int copy_d2h(tups_ctx* ctx, void* host, const void* dev, size_t bytes) {
+  if (!host) return tups::set_error(ctx, TUPS_ERR_BADARG, "NULL host buffer");
+  TRY(tups::cuda_check(ctx, cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, ctx->stream), "D2H"));
+  return tups::cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "synchronize");
+}
+
+int copy_h2d(tups_ctx* ctx, void* dev, const void* host, size_t bytes) {
+  if (!host) return tups::set_error(ctx, TUPS_ERR_BADARG, "NULL host buffer");
+  TRY(tups::cuda_check(ctx, cudaMemcpyAsync(dev, host, bytes, cudaMemcpyHostToDevice, ctx->stream), "H2D"));
+  return tups::cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "synchronize");
+}
+
+int green_async(tups_ctx* ctx, int cal_chi) {
+  TRY(tups::launch_sigma_hartree(ctx));
+  TRY(tups::launch_bisection(ctx, cal_chi, kMuMaxSteps));
+  TRY(tups::launch_grt(ctx));
+  TRY(tups::launch_gkw(ctx));
+  ctx->have_green = true;
+  return TUPS_OK;
+}
+
+int bse_async(tups_ctx* ctx) {
+  if (!ctx->have_green) return tups::set_error(ctx, TUPS_ERR_STATE, "BSE before calc_Gkw_Grt");
+  const int Nb = ctx->d.Nb;
+  const int chunk_q = (int)std::max<size_t>(1, ctx->s.bse_chunk / 4);
+  for (int q0 = 0; q0 < Nb; q0 += chunk_q) {
+    const int nq = std::min(chunk_q, Nb - q0);
+    TRY(tups::launch_chi(ctx, q0, nq));
+    TRY(tups::launch_bse_chunk(ctx, q0, nq));
+  }
+  return TUPS_OK;
+}
+
+int sde_async(tups_ctx* ctx) {
+  if (!ctx->have_green) return tups::set_error(ctx, TUPS_ERR_STATE, "calc_SDE before calc_Gkw_Grt");
+  const size_t bytes = (size_t)ctx->d.Nt * sizeof(cplx);
+  TRY(tups::cuda_check(ctx,
+                       cudaMemcpyAsync(ctx->s.SigmaOld, ctx->s.Sigma, bytes, cudaMemcpyDeviceToDevice, ctx->stream),
+                       "SigmaOld = Sigma"));
+  return tups::launch_sde(ctx);
+}
+
+}  // namespace
+
+extern "C" int tups_calc_Gkw_Grt(tups_ctx* ctx, int ite, int cal_chi) {
+  (void)ite;
+  if (!ctx) return TUPS_ERR_BADARG;
+  TRY(set_dev(ctx));
+  TRY(green_async(ctx, cal_chi));
+  return device_status(ctx);
+}
+
+extern "C" int tups_calc_chi(tups_ctx* ctx, int idx_q, double* chi_ph_LL, double* chi_pp_LL) {
+  if (!ctx) return TUPS_ERR_BADARG;
+  const auto& d = ctx->d;
+  if (idx_q < 1 || idx_q > d.Nb) return tups::set_error(ctx, TUPS_ERR_BADARG, "idx_q out of range");
+  if (!ctx->have_green) return tups::set_error(ctx, TUPS_ERR_STATE, "calc_chi before calc_Gkw_Grt");
+  TRY(set_dev(ctx));
+  TRY(tups::launch_chi(ctx, idx_q - 1, 1));
+  const size_t nb = (size_t)d.Nl * d.Nl * d.Nf;
+  std::vector<cplx> ph(nb), pp(nb);
+  TRY(copy_d2h(ctx, ph.data(), ctx->s.chi_ph + nb * (idx_q - 1), nb * sizeof(cplx)));
+  TRY(copy_d2h(ctx, pp.data(), ctx->s.chi_pp + nb * (idx_q - 1), nb * sizeof(cplx)));
+  const size_t Nz = d.Nz;
+  for (int which = 0; which < 2; which++) {
+    double* out = which == 0 ? chi_ph_LL : chi_pp_LL;
+    if (!out) continue;
+    const std::vector<cplx>& src = which == 0 ? ph : pp;
+    std::memset(out, 0, 2 * Nz * Nz * sizeof(double));
+    for (int nu = 0; nu < d.Nf; nu++)
+      for (int l2 = 0; l2 < d.Nl; l2++)
+        for (int l1 = 0; l1 < d.Nl; l1++) {
+          const cplx v = src[l1 + (size_t)d.Nl * (l2 + (size_t)d.Nl * nu)];
+          const size_t o = (size_t)(l1 * d.Nf + nu) + Nz * (size_t)(l2 * d.Nf + nu);
+          out[2 * o] = v.x;
+          out[2 * o + 1] = v.y;
+        }
+  }
+  return TUPS_OK;
+}
+
+extern "C" int tups_BSE(tups_ctx* ctx, int ite) {
+  (void)ite;
+  if (!ctx) return TUPS_ERR_BADARG;
+  TRY(set_dev(ctx));
+  TRY(bse_async(ctx));
+  return tups::cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "BSE");
+}
+
+extern "C" int tups_calc_PhiR(tups_ctx* ctx, int ite) {
+  (void)ite;
+  if (!ctx) return TUPS_ERR_BADARG;
+  if (!ctx->have_exp) return tups::set_error(ctx, TUPS_ERR_STATE, "calc_PhiR before calculate_expSqR");
+  TRY(set_dev(ctx));
+  TRY(tups::launch_phir(ctx));
+  ctx->have_phir = true;
+  return tups::cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "calc_PhiR");
+}
+
+static int calc_M(tups_ctx* ctx, int which) {
+  if (!ctx) return TUPS_ERR_BADARG;
+  TRY(set_dev(ctx));
+  TRY(tups::launch_M(ctx, which));
+  ctx->have_M = true;
+  return TUPS_OK;
+}
+extern "C" int tups_calc_M_phbar_to_ph(tups_ctx* ctx) { return calc_M(ctx, 0); }
+extern "C" int tups_calc_M_pp_to_ph(tups_ctx* ctx) { return calc_M(ctx, 1); }
+extern "C" int tups_calc_M_ph_to_pp(tups_ctx* ctx) { return calc_M(ctx, 2); }
+extern "C" int tups_calc_M_phbar_to_pp(tups_ctx* ctx) { return calc_M(ctx, 3); }
+
+extern "C" int tups_calculate_PAE(tups_ctx* ctx) {
+  if (!ctx) return TUPS_ERR_BADARG;
+  if (!ctx->have_M || !ctx->have_phir)
+    return tups::set_error(ctx, TUPS_ERR_STATE, "calculate_PAE before calc_PhiR / calc_M_*");
+  TRY(set_dev(ctx));
+  TRY(tups::launch_pae(ctx));
+  return tups::cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "calculate_PAE");
+}
+
+extern "C" int tups_calc_SDE(tups_ctx* ctx, int ite) {
+  (void)ite;
+  if (!ctx) return TUPS_ERR_BADARG;
+  TRY(set_dev(ctx));
+  TRY(sde_async(ctx));
+  return tups::cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "calc_SDE");
+}
+
+extern "C" int tups_conv(tups_ctx* ctx, tups_conv_info* info) {
+  if (!ctx) return TUPS_ERR_BADARG;
+  TRY(set_dev(ctx));
+  TRY(tups::launch_conv(ctx));
+  double sc[tups::S_COUNT];
+  TRY(read_scalars(ctx, sc));
+  tups_conv_info ci;
+  std::memset(&ci, 0, sizeof(ci));
+  ci.rel_sig_max = sc[tups::S_RELSIG];
+  ci.rel_sig_av = sc[tups::S_RELSIGAV];
+  ci.dsigma_inf = sc[tups::S_DSIG];
+  ci.mu = sc[tups::S_MU];
+  ci.bisection_steps = (int)sc[tups::S_STEPS];
+  // f_sigma = f_vert = real(1e-8, 8) (SRC/parquet_ini.f90:31-32)
+  const double f_tol = (double)1e-8f;
+  bool ok = ci.rel_sig_max < f_tol;
+  for (int r = 0; r < 4; r++) {
+    ci.F_max[r] = sc[tups::S_FMAX + r];
+    const double prev = ctx->F_max_prev[r];
+    ci.rel_err[r] = prev != 0.0 ? std::fabs(1.0 - ci.F_max[r] / prev) : INFINITY;
+    ok = ok && ci.rel_err[r] < f_tol;
+    ctx->F_max_prev[r] = ci.F_max[r];
+  }
+  if (ctx->p.conv_abs > 0.0) ok = ci.dsigma_inf < ctx->p.conv_abs;
+  ci.converged = ok ? 1 : 0;
+  const size_t bytes = (size_t)ctx->d.Nt * sizeof(cplx);
+  TRY(tups::cuda_check(ctx,
+                       cudaMemcpyAsync(ctx->s.SigmaOld, ctx->s.Sigma, bytes, cudaMemcpyDeviceToDevice, ctx->stream),
+                       "SigmaOld = Sigma"));
+  if (info) *info = ci;
+  if (sc[tups::S_NANFLAG] > 0.0 || !std::isfinite(ci.rel_sig_max))
+    return tups::set_error(ctx, TUPS_ERR_NAN, "NaN or Inf in the self-energy or a vertex");
+  return TUPS_OK;
+}
+
+extern "C" int tups_vertex_update(tups_ctx* ctx) {
+  if (!ctx) return TUPS_ERR_BADARG;
+  TRY(set_dev(ctx));
+  TRY(tups::launch_vertex_update(ctx));
+  return tups::cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "vertex update");
+}
+
+extern "C" int tups_output_block(tups_ctx* ctx) {
+  if (!ctx) return TUPS_ERR_BADARG;
+  TRY(set_dev(ctx));
+  return tups::launch_output_mu(ctx);
+}
+
+extern "C" int tups_iteration(tups_ctx* ctx, int ite, tups_conv_info* info) {
+  if (!ctx) return TUPS_ERR_BADARG;
+  TRY(set_dev(ctx));
+  // SRC/loop.f90:67 .. 222, without the HDF5 output
+  TRY(green_async(ctx, 0));
+  TRY(bse_async(ctx));
+  if (ite == 0 || !ctx->have_exp) {
+    TRY(tups_calculate_expSqR(ctx));
+    TRY(tups_calculate_expqSR(ctx));
+  }
+  TRY(tups::launch_phir(ctx));
+  ctx->have_phir = true;
+  if (ite == 0 || !ctx->have_M)
+    for (int w = 0; w < 4; w++) TRY(calc_M(ctx, w));
+  TRY(tups::launch_pae(ctx));
+  if (!ctx->p.oneshot || ite == ctx->p.ite_max - 1) TRY(sde_async(ctx));
+  TRY(device_status(ctx));
+  tups_conv_info ci;
+  int rc = tups_conv(ctx, &ci);
+  if (info) *info = ci;
+  if (rc) return rc;
+  if (ite % 5 == 0 || ite == ctx->p.ite_max - 1 || ci.converged) TRY(tups::launch_output_mu(ctx));
+  TRY(tups::launch_vertex_update(ctx));
+  return TUPS_OK;
+}
+
+extern "C" int tups_execute_loop(tups_ctx* ctx, int* ite_out, int* converged) {
+  if (!ctx) return TUPS_ERR_BADARG;
+  int ite = 0, conv = 0;
+  while (!conv && ite < ctx->p.ite_max) {
+    tups_conv_info ci;
+    int rc = tups_iteration(ctx, ite, &ci);
+    if (rc) {
+      if (ite_out) *ite_out = ite;
+      return rc;
+    }
+    conv = ci.converged;
+    ite++;
+  }
+  if (ite_out) *ite_out = ite;
+  if (converged) *converged = conv;
+  return tups::cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "execute_loop");
+}
+
+// ---- state in/out -----------------------------------------------------------
+extern "C" int tups_get_sigma(tups_ctx* ctx, double* h) {
+  if (!ctx) return TUPS_ERR_BADARG;
+  return copy_d2h(ctx, h, ctx->s.Sigma, (size_t)ctx->d.Nt * sizeof(cplx));
+}
+extern "C" int tups_set_sigma(tups_ctx* ctx, const double* h) {
+  if (!ctx) return TUPS_ERR_BADARG;
+  return copy_h2d(ctx, ctx->s.Sigma, h, (size_t)ctx->d.Nt * sizeof(cplx));
+}
+extern "C" int tups_get_sigma_old(tups_ctx* ctx, double* h) {
+  if (!ctx) return TUPS_ERR_BADARG;
+  return copy_d2h(ctx, h, ctx->s.SigmaOld, (size_t)ctx->d.Nt * sizeof(cplx));
+}
+extern "C" int tups_get_Gkw(tups_ctx* ctx, double* h) {
+  if (!ctx) return TUPS_ERR_BADARG;
+  return copy_d2h(ctx, h, ctx->s.Gkw, (size_t)ctx->d.Nt * sizeof(cplx));
+}
+extern "C" int tups_get_Grt(tups_ctx* ctx, double* h) {
+  if (!ctx) return TUPS_ERR_BADARG;
+  const auto& d = ctx->d;
+  return copy_d2h(ctx, h, ctx->s.Grt, (size_t)d.Nx * d.Ngrain * d.Ny * d.Ngrain * d.Nf * sizeof(cplx));
+}
+extern "C" int tups_get_mu(tups_ctx* ctx, double* mu) {
+  if (!ctx || !mu) return TUPS_ERR_BADARG;
+  return copy_d2h(ctx, mu, ctx->s.scal + tups::S_MU, sizeof(double));
+}
+extern "C" int tups_set_mu(tups_ctx* ctx, double mu) {
+  if (!ctx) return TUPS_ERR_BADARG;
+  return copy_h2d(ctx, ctx->s.scal + tups::S_MU, &mu, sizeof(double));
+}
+static cplx* vertex_ptr(tups_ctx* ctx, int channel, int which) {
+  if (channel < 0 || channel > 3 || which < 0 || which > 1) return nullptr;
+  return which == 0 ? ctx->s.F[channel] : ctx->s.G[channel];
+}
+extern "C" int tups_get_vertex(tups_ctx* ctx, int channel, int which, double* h) {
+  if (!ctx) return TUPS_ERR_BADARG;
+  cplx* p = vertex_ptr(ctx, channel, which);
+  if (!p) return tups::set_error(ctx, TUPS_ERR_BADARG, "channel/which out of range");
+  const auto& d = ctx->d;
+  return copy_d2h(ctx, h, p, (size_t)d.Nz * d.Nz * d.Nb * sizeof(cplx));
+}
+extern "C" int tups_set_vertex(tups_ctx* ctx, int channel, int which, const double* h) {
+  if (!ctx) return TUPS_ERR_BADARG;
+  cplx* p = vertex_ptr(ctx, channel, which);
+  if (!p) return tups::set_error(ctx, TUPS_ERR_BADARG, "channel/which out of range");
+  const auto& d = ctx->d;
+  return copy_h2d(ctx, p, h, (size_t)d.Nz * d.Nz * d.Nb * sizeof(cplx));
+}
+extern "C" int tups_get_PhiR(tups_ctx* ctx, int channel, double* h) {
+  if (!ctx || channel < 0 || channel > 3) return TUPS_ERR_BADARG;
+  const auto& d = ctx->d;
+  return copy_d2h(ctx, h, ctx->s.PhiR[channel], (size_t)d.Nz * d.Nz * (d.Nf / 2) * d.NR * sizeof(cplx));
+}
+extern "C" int tups_get_M(tups_ctx* ctx, int which, double* h) {
+  if (!ctx || which < 0 || which > 3 || !h) return TUPS_ERR_BADARG;
+  const auto& d = ctx->d;
+  const size_t nl4 = (size_t)d.Nl * d.Nl * d.Nl * d.Nl;
+  std::vector<cplx> m(nl4 * d.NIBZ * d.NR);
+  TRY(copy_d2h(ctx, m.data(), ctx->s.M[which], m.size() * sizeof(cplx)));
+  cplx* out = reinterpret_cast<cplx*>(h);
+  for (int R = 0; R < d.NR; R++)
+    for (int q = 0; q < d.Nb; q++) {
+      const int Qi = q / (d.Nf / 2);
+      std::memcpy(out + nl4 * (q + (size_t)d.Nb * R), m.data() + nl4 * (Qi + (size_t)d.NIBZ * R), nl4 * sizeof(cplx));
+    }
+  return TUPS_OK;
+}
+extern "C" int tups_get_expSqR(tups_ctx* ctx, double* h) {
+  if (!ctx) return TUPS_ERR_BADARG;
+  const auto& d = ctx->d;
+  return copy_d2h(ctx, h, ctx->t.expSqR, (size_t)d.NIBZ * d.NR * tups::NS * sizeof(cplx));
+}
+extern "C" int tups_get_expqSR(tups_ctx* ctx, double* h) {
+  if (!ctx) return TUPS_ERR_BADARG;
+  const auto& d = ctx->d;
+  return copy_d2h(ctx, h, ctx->t.expqSR, (size_t)d.Nc * d.NR * tups::NS * sizeof(cplx));
+}
+extern "C" int tups_get_sde_aux(tups_ctx* ctx, double* cph, double* cpp, double* lchi, double* phchi,
+                                double* ppchi) {
+  if (!ctx) return TUPS_ERR_BADARG;
+  const auto& d = ctx->d;
+  const size_t na = (size_t)d.Nl * d.nbox * d.Nb * sizeof(cplx), nz = (size_t)d.Nz * d.Nb * sizeof(cplx);
+  if (cph) TRY(copy_d2h(ctx, cph, ctx->s.chi_aux_ph, na));
+  if (cpp) TRY(copy_d2h(ctx, cpp, ctx->s.chi_aux_pp, na));
+  if (lchi) TRY(copy_d2h(ctx, lchi, ctx->s.LChi, nz));
+  if (phchi) TRY(copy_d2h(ctx, phchi, ctx->s.PhChi, nz));
+  if (ppchi) TRY(copy_d2h(ctx, ppchi, ctx->s.PPChi, nz));
+  return TUPS_OK;
+}
+extern "C" int tups_synchronize(tups_ctx* ctx) {
+  if (!ctx) return TUPS_ERR_BADARG;
+  return tups::cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "synchronize");
+}

@@ -1,0 +1,246 @@
+// Bethe-Salpeter step, BSE(ite) (SRC/parquet_BSE.f90:19-135).
+//
+// Per bosonic slot q and channel r the reference computes, with four ZGEMMs,
+//   Phi_r = c_r f [ (a Gamma chi) F + F (a chi Gamma) ] + (1-f)(F - Gamma),
+// a = 1/(beta Nx Ny), c_d = c_m = 1/2 (chi_ph), c_s = -1/4, c_t = +1/4 (chi_pp).
+// chi is block-diagonal in nu (one Nl x Nl block per nu), so Gamma chi and
+// chi Gamma cost Nz^2 Nl each (k_bse_prep).  The remaining work is ONE complex
+// GEMM with K = 2 Nz,  [Gamma chi | F] x [F ; chi Gamma],  run on the FP64
+// tensor cores (mma.sync m16n8k8 f64, k_bse_gemm) with the scale and the
+// damping term fused into the epilogue; Phi_r overwrites Gamma_r in place.
+#include "tups_device.cuh"
+
+namespace tups {
+
+struct BsePtrs {
+  cplx* F[4];
+  cplx* G[4];
+  double scale[4];  // c_r * f * a
+};
+
+// A = Gamma chi and B = chi Gamma for the instances (q, r) of one chunk;
+// instance = (q - q_begin) * 4 + r.  Column-major (Nz, Nz), row = l*Nf + nu.
+__global__ void k_bse_prep(BsePtrs P, const cplx* __restrict__ chi_ph, const cplx* __restrict__ chi_pp,
+                           cplx* __restrict__ A, cplx* __restrict__ B, int q_begin, int Nz, int Nf, int Nl) {
+  const int inst = blockIdx.y;
+  const int q = q_begin + inst / 4, r = inst % 4;
+  const cplx* chi = (r < 2 ? chi_ph : chi_pp) + (size_t)Nl * Nl * Nf * q;
+  const cplx* Gm = P.G[r] + (size_t)Nz * Nz * q;
+  cplx* Ai = A + (size_t)Nz * Nz * inst;
+  cplx* Bi = B + (size_t)Nz * Nz * inst;
+  const size_t n2 = (size_t)Nz * Nz;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n2; e += (size_t)gridDim.x * blockDim.x) {
+    int row = (int)(e % Nz), col = (int)(e / Nz);
+    // A[row, (l2, nu)] = sum_l1 Gamma[row, (l1, nu)] chi[l1, l2, nu]
+    {
+      int l2 = col / Nf, nu = col % Nf;
+      cplx acc = cmk(0.0, 0.0);
+      for (int l1 = 0; l1 < Nl; l1++)
+        acc = cfma(Gm[row + (size_t)Nz * (l1 * Nf + nu)], chi[l1 + Nl * (l2 + (size_t)Nl * nu)], acc);
+      Ai[e] = acc;
+    }
+    // B[(l1, nu), col] = sum_l2 chi[l1, l2, nu] Gamma[(l2, nu), col]
+    {
+      int l1 = row / Nf, nu = row % Nf;
+      cplx acc = cmk(0.0, 0.0);
+      for (int l2 = 0; l2 < Nl; l2++)
+        acc = cfma(chi[l1 + Nl * (l2 + (size_t)Nl * nu)], Gm[(l2 * Nf + nu) + (size_t)Nz * col], acc);
+      Bi[e] = acc;
+    }
+  }
+}
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc, bool valid) {
+  unsigned sz = valid ? 16u : 0u;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(sdst)), "l"(gsrc), "r"(sz));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+// D += A*B on 16x8x8 f64 tiles (row.col): a[4], b[2], c[4] per thread
+__device__ __forceinline__ void dmma16x8x8(double* c, const double* a, const double* b) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
+}
+
+// Batched complex GEMM on the FP64 tensor cores with the BSE epilogue.
+// CTA tile BM x BN (complex), K step BK; WM x WN warps, warp tile
+// (16 TM) x (8 TN).  Left operand L = [A | F] (Nz x 2Nz), right R = [F ; B].
+template <int BM, int BN, int BK, int WM, int WN, int STAGES>
+__global__ void __launch_bounds__(WM* WN * 32) k_bse_gemm(BsePtrs P, const cplx* __restrict__ A,
+                                                          const cplx* __restrict__ B, int q_begin, int Nz,
+                                                          double one_minus_f) {
+  constexpr int TM = BM / WM / 16, TN = BN / WN / 8;
+  constexpr int LDL = BM + 2;  // conflict-free 16-byte fragment loads
+  constexpr int LDR = BK + 4;
+  constexpr int NT = WM * WN * 32;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  cplx* sL = reinterpret_cast<cplx*>(smraw);           // [STAGES][BK][LDL]
+  cplx* sR = sL + (size_t)STAGES * BK * LDL;           // [STAGES][BN][LDR]
+
+  const int inst = blockIdx.y;
+  const int q = q_begin + inst / 4, r = inst % 4;
+  const size_t n2 = (size_t)Nz * Nz;
+  const cplx* Ai = A + n2 * inst;
+  const cplx* Bi = B + n2 * inst;
+  const cplx* Fq = P.F[r] + n2 * q;
+  cplx* Gq = P.G[r] + n2 * q;
+  const int tiles_m = (Nz + BM - 1) / BM;
+  const int m0 = (blockIdx.x % tiles_m) * BM, n0 = (blockIdx.x / tiles_m) * BN;
+  const int K = 2 * Nz;
+  const int ktiles = (K + BK - 1) / BK;
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm0 = (warp % WM) * (16 * TM), wn0 = (warp / WM) * (8 * TN);
+  const int gid = lane >> 2, tig = lane & 3;
+
+  auto load_stage = [&](int stage, int kt) {
+    const int k0 = kt * BK;
+    cplx* dL = sL + (size_t)stage * BK * LDL;
+    cplx* dR = sR + (size_t)stage * BN * LDR;
+    for (int e = tid; e < BK * BM; e += NT) {
+      int m = e % BM, kk = e / BM;
+      int gm = m0 + m, gk = k0 + kk;
+      bool ok = gm < Nz && gk < K;
+      const cplx* src = Ai;
+      if (ok) src = gk < Nz ? Ai + gm + (size_t)Nz * gk : Fq + gm + (size_t)Nz * (gk - Nz);
+      cp_async16(dL + kk * LDL + m, src, ok);
+    }
+    for (int e = tid; e < BK * BN; e += NT) {
+      int kk = e % BK, n = e / BK;
+      int gn = n0 + n, gk = k0 + kk;
+      bool ok = gn < Nz && gk < K;
+      const cplx* src = Fq;
+      if (ok) src = gk < Nz ? Fq + gk + (size_t)Nz * gn : Bi + (gk - Nz) + (size_t)Nz * gn;
+      cp_async16(dR + n * LDR + kk, src, ok);
+    }
+  };
+
+  double cre[TM][TN][4], cim[TM][TN][4];
+#pragma unroll
+  for (int i = 0; i < TM; i++)
+#pragma unroll
+    for (int j = 0; j < TN; j++)
+#pragma unroll
+      for (int e = 0; e < 4; e++) cre[i][j][e] = cim[i][j][e] = 0.0;
+
+#pragma unroll
+  for (int s = 0; s < STAGES - 1; s++) {
+    if (s < ktiles) load_stage(s, s);
+    cp_async_commit();
+  }
+  for (int kt = 0; kt < ktiles; kt++) {
+    cp_async_wait<STAGES - 2>();
+    __syncthreads();
+    {
+      int nk = kt + STAGES - 1;
+      if (nk < ktiles) load_stage(nk % STAGES, nk);
+      cp_async_commit();
+    }
+    const cplx* cL = sL + (size_t)(kt % STAGES) * BK * LDL;
+    const cplx* cR = sR + (size_t)(kt % STAGES) * BN * LDR;
+#pragma unroll
+    for (int k8 = 0; k8 < BK; k8 += 8) {
+      double are[TM][4], aim[TM][4], anim[TM][4], bre[TN][2], bim[TN][2];
+#pragma unroll
+      for (int i = 0; i < TM; i++) {
+        const int mb = wm0 + i * 16 + gid;
+        cplx v0 = cL[(k8 + tig) * LDL + mb];
+        cplx v1 = cL[(k8 + tig) * LDL + mb + 8];
+        cplx v2 = cL[(k8 + tig + 4) * LDL + mb];
+        cplx v3 = cL[(k8 + tig + 4) * LDL + mb + 8];
+        are[i][0] = v0.x; aim[i][0] = v0.y;
+        are[i][1] = v1.x; aim[i][1] = v1.y;
+        are[i][2] = v2.x; aim[i][2] = v2.y;
+        are[i][3] = v3.x; aim[i][3] = v3.y;
+#pragma unroll
+        for (int e = 0; e < 4; e++) anim[i][e] = -aim[i][e];
+      }
+#pragma unroll
+      for (int j = 0; j < TN; j++) {
+        const int nb = wn0 + j * 8 + gid;
+        cplx w0 = cR[nb * LDR + k8 + tig];
+        cplx w1 = cR[nb * LDR + k8 + tig + 4];
+        bre[j][0] = w0.x; bim[j][0] = w0.y;
+        bre[j][1] = w1.x; bim[j][1] = w1.y;
+      }
+#pragma unroll
+      for (int i = 0; i < TM; i++)
+#pragma unroll
+        for (int j = 0; j < TN; j++) {
+          dmma16x8x8(cre[i][j], are[i], bre[j]);
+          dmma16x8x8(cre[i][j], anim[i], bim[j]);
+          dmma16x8x8(cim[i][j], are[i], bim[j]);
+          dmma16x8x8(cim[i][j], aim[i], bre[j]);
+        }
+    }
+  }
+  cp_async_wait<0>();
+
+  // epilogue: Phi = s * C + (1-f) (F - Gamma), written over Gamma
+  const double s = P.scale[r];
+#pragma unroll
+  for (int i = 0; i < TM; i++)
+#pragma unroll
+    for (int j = 0; j < TN; j++)
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        int row = m0 + wm0 + i * 16 + gid + (e >= 2 ? 8 : 0);
+        int col = n0 + wn0 + j * 8 + 2 * tig + (e & 1);
+        if (row < Nz && col < Nz) {
+          size_t idx = row + (size_t)Nz * col;
+          cplx f = Fq[idx], g = Gq[idx];
+          Gq[idx] = cmk(s * cre[i][j][e] + one_minus_f * (f.x - g.x), s * cim[i][j][e] + one_minus_f * (f.y - g.y));
+        }
+      }
+}
+
+template <int BM, int BN, int BK, int WM, int WN, int STAGES>
+static int run_gemm(tups_ctx* ctx, const BsePtrs& P, int q_begin, int q_count) {
+  const int Nz = ctx->d.Nz;
+  constexpr int LDL = BM + 2, LDR = BK + 4;
+  size_t sm = (size_t)STAGES * (BK * LDL + BN * LDR) * sizeof(cplx);
+  auto kern = k_bse_gemm<BM, BN, BK, WM, WN, STAGES>;
+  if (sm > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return cuda_check(ctx, e, "k_bse_gemm smem attribute");
+  }
+  int tiles = ((Nz + BM - 1) / BM) * ((Nz + BN - 1) / BN);
+  dim3 grid(tiles, 4 * q_count);
+  kern<<<grid, WM * WN * 32, sm, ctx->stream>>>(P, ctx->s.bse_A, ctx->s.bse_B, q_begin, Nz,
+                                                1.0 - ctx->p.f_damping);
+  return after_launch(ctx, "k_bse_gemm");
+}
+
+int launch_bse_chunk(tups_ctx* ctx, int q_begin, int q_count) {
+  const auto& d = ctx->d;
+  BsePtrs P;
+  const double a = 1.0 / (ctx->p.beta * d.Nx * d.Ny);
+  const double c[4] = {0.5, 0.5, -0.25, 0.25};
+  for (int r = 0; r < 4; r++) {
+    P.F[r] = ctx->s.F[r];
+    P.G[r] = ctx->s.G[r];
+    P.scale[r] = c[r] * ctx->p.f_damping * a;
+  }
+  const size_t n2 = (size_t)d.Nz * d.Nz;
+  dim3 pgrid((unsigned)std::min<size_t>(cdiv(n2, 256), 4096), 4 * q_count);
+  k_bse_prep<<<pgrid, 256, 0, ctx->stream>>>(P, ctx->s.chi_ph, ctx->s.chi_pp, ctx->s.bse_A, ctx->s.bse_B, q_begin,
+                                             d.Nz, d.Nf, d.Nl);
+  int rc = after_launch(ctx, "k_bse_prep");
+  if (rc) return rc;
+  // tile choice: 64x64 when Nz is a multiple of 64 (or large), else 32x32
+  if (d.Nz % 64 == 0 || d.Nz > 512) return run_gemm<64, 64, 16, 2, 2, 3>(ctx, P, q_begin, q_count);
+  if (d.Nz >= 32) return run_gemm<32, 32, 16, 2, 2, 3>(ctx, P, q_begin, q_count);
+  return run_gemm<16, 16, 16, 1, 2, 3>(ctx, P, q_begin, q_count);
+}
+
+}  // namespace tups

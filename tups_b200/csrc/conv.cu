@@ -1,0 +1,98 @@
+// Convergence check conv() (SRC/parquet_check.f90:39-150) and the vertex
+// update Gamma_r = F_r - Phi_r (SRC/loop.f90:219-222).
+#include "tups_device.cuh"
+
+namespace tups {
+
+// Sigma part of conv(): max and mean of |SigmaOld - Sigma|/|Sigma|, max
+// |SigmaOld - Sigma|, NaN/Inf flag.  One CTA.
+__global__ void __launch_bounds__(1024) k_conv_sigma(const cplx* __restrict__ S, const cplx* __restrict__ So,
+                                                     double* scal, int Nt) {
+  __shared__ double sh[32];
+  double mx = 0.0, sum = 0.0, dmx = 0.0, bad = 0.0;
+  for (int i = threadIdx.x; i < Nt; i += blockDim.x) {
+    const cplx a = S[i], b = So[i];
+    const double dx = b.x - a.x, dy = b.y - a.y;
+    const double d = sqrt(dx * dx + dy * dy);
+    const double rel = d / sqrt(a.x * a.x + a.y * a.y);
+    if (!isfinite(a.x) || !isfinite(a.y)) bad = 1.0;
+    mx = fmax(mx, rel);
+    dmx = fmax(dmx, d);
+    sum += rel;
+  }
+  mx = warp_max(mx);
+  dmx = warp_max(dmx);
+  bad = warp_max(bad);
+  __shared__ double smx[32], sdm[32], sbd[32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) {
+    smx[wid] = mx;
+    sdm[wid] = dmx;
+    sbd[wid] = bad;
+  }
+  sum = block_sum(sum, sh);
+  if (threadIdx.x == 0) {
+    double a = 0.0, b = 0.0, c = 0.0;
+    for (int w = 0; w < (int)(blockDim.x + 31) / 32; w++) {
+      a = fmax(a, smx[w]);
+      b = fmax(b, sdm[w]);
+      c = fmax(c, sbd[w]);
+    }
+    scal[S_RELSIG] = a;
+    scal[S_RELSIGAV] = fabs(sum / Nt);
+    scal[S_DSIG] = b;
+    scal[S_NANFLAG] = c;
+    for (int r = 0; r < 4; r++) scal[S_FMAX + r] = 0.0;
+  }
+}
+
+// max |F_r| for the four channels; grid-stride, atomic max of per-CTA maxima
+__global__ void k_fmax(const cplx* __restrict__ F0, const cplx* __restrict__ F1, const cplx* __restrict__ F2,
+                       const cplx* __restrict__ F3, size_t n, double* scal) {
+  const cplx* F = blockIdx.y == 0 ? F0 : (blockIdx.y == 1 ? F1 : (blockIdx.y == 2 ? F2 : F3));
+  double mx = 0.0, bad = 0.0;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const cplx v = F[i];
+    const double a2 = v.x * v.x + v.y * v.y;
+    if (!isfinite(a2)) bad = 1.0;
+    mx = fmax(mx, a2);
+  }
+  mx = warp_max(mx);
+  bad = warp_max(bad);
+  if ((threadIdx.x & 31) == 0) {
+    atomic_max_nonneg(&scal[S_FMAX + blockIdx.y], sqrt(mx));
+    if (bad > 0.0) atomic_max_nonneg(&scal[S_NANFLAG], 1.0);
+  }
+}
+
+// G_r = F_r - G_r for the four channels
+__global__ void k_vertex_update(cplx* __restrict__ G0, cplx* __restrict__ G1, cplx* __restrict__ G2,
+                                cplx* __restrict__ G3, const cplx* __restrict__ F0, const cplx* __restrict__ F1,
+                                const cplx* __restrict__ F2, const cplx* __restrict__ F3, size_t n) {
+  cplx* G = blockIdx.y == 0 ? G0 : (blockIdx.y == 1 ? G1 : (blockIdx.y == 2 ? G2 : G3));
+  const cplx* F = blockIdx.y == 0 ? F0 : (blockIdx.y == 1 ? F1 : (blockIdx.y == 2 ? F2 : F3));
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    G[i] = csub(F[i], G[i]);
+}
+
+int launch_conv(tups_ctx* ctx) {
+  const auto& d = ctx->d;
+  k_conv_sigma<<<1, 1024, 0, ctx->stream>>>(ctx->s.Sigma, ctx->s.SigmaOld, ctx->s.scal, d.Nt);
+  int rc = after_launch(ctx, "k_conv_sigma");
+  if (rc) return rc;
+  const size_t n = (size_t)d.Nz * d.Nz * d.Nb;
+  dim3 grid((unsigned)std::min<size_t>(cdiv(n, 256), 148 * 8), 4);
+  k_fmax<<<grid, 256, 0, ctx->stream>>>(ctx->s.F[0], ctx->s.F[1], ctx->s.F[2], ctx->s.F[3], n, ctx->s.scal);
+  return after_launch(ctx, "k_fmax");
+}
+
+int launch_vertex_update(tups_ctx* ctx) {
+  const auto& d = ctx->d;
+  const size_t n = (size_t)d.Nz * d.Nz * d.Nb;
+  dim3 grid((unsigned)std::min<size_t>(cdiv(n, 256), 148 * 8), 4);
+  k_vertex_update<<<grid, 256, 0, ctx->stream>>>(ctx->s.G[0], ctx->s.G[1], ctx->s.G[2], ctx->s.G[3], ctx->s.F[0],
+                                                 ctx->s.F[1], ctx->s.F[2], ctx->s.F[3], n);
+  return after_launch(ctx, "k_vertex_update");
+}
+
+}  // namespace tups

@@ -1,0 +1,125 @@
+// Internal declarations shared by the host runtime and the kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/tups_b200.h"
+
+namespace tups {
+
+constexpr int NS = 8;  // point-group operations of the square lattice
+
+// complex128 as interleaved doubles on the device
+typedef double2 cplx;
+
+struct DeviceTables {
+  double* FF = nullptr;       // (Nx, Ny, Nl) column-major
+  double* FF_inv = nullptr;   // (8, Nx, Ny, Nl)
+  double* Ek = nullptr;       // (Nx, Ny)
+  double* Ekg = nullptr;      // (Ng, Ng, Nx, Ny)
+  int* signs = nullptr;       // (Nl)
+  int* lsym = nullptr;        // (8, Nl), 0-based target l
+  double* lfac = nullptr;     // (8, Nl)
+  int* ibz = nullptr;         // (Nred, 3): qx, qy, w (1-based)
+  int* symlist = nullptr;     // (NIBZ, 8) 0/1
+  int* symq = nullptr;        // (NIBZ, 8, 2): S(q) 1-based (qx, qy)
+  cplx* L[4] = {};            // Lambda_r (Nf, Nf, Nf/2)
+  cplx* expSqR = nullptr;     // (NIBZ, NR, 8)
+  cplx* expqSR = nullptr;     // (Nc, NR, 8), k index (ky-1)*Nx+kx
+  cplx* tw_tau = nullptr;     // (Nf tau, Nf nu) e^{-i nu_n tau_i}
+  cplx* tw_x = nullptr;       // (Nx*Ng) e^{-2 pi i m / n1}
+  cplx* tw_y = nullptr;       // (Ny*Ng)
+};
+
+struct DeviceState {
+  cplx* Sigma = nullptr;      // (Nt)
+  cplx* SigmaOld = nullptr;   // (Nt)
+  cplx* SigmaH = nullptr;     // (Nx, Ny)
+  cplx* Gkw = nullptr;        // (Nt)
+  cplx* Grt = nullptr;        // (Nx*Ng, Ny*Ng, Nf)
+  cplx* Grt_work = nullptr;   // same size, FFT scratch
+  cplx* F[4] = {};            // (Nz, Nz, Nb)
+  cplx* G[4] = {};            // (Nz, Nz, Nb)
+  cplx* chi_ph = nullptr;     // (Nl, Nl, Nf, Nb) nu-diagonal blocks of chi_ph_LL
+  cplx* chi_pp = nullptr;
+  cplx* bse_A = nullptr;      // BSE scratch: Gamma*chi per instance of a chunk
+  cplx* bse_B = nullptr;      // chi*Gamma
+  size_t bse_chunk = 0;       // instances per chunk
+  cplx* PhiR[4] = {};         // (Nz*Nz, Nf/2, NR)
+  cplx* M[4] = {};            // (Nl^4, NIBZ, NR): 0 phbar_to_ph 1 pp_to_ph 2 ph_to_pp 3 phbar_to_pp
+  cplx* chi_aux_ph = nullptr; // (Nl*nbox, Nb)
+  cplx* chi_aux_pp = nullptr;
+  cplx* LChi = nullptr;       // (Nz, Nb)
+  cplx* PhChi = nullptr;
+  cplx* PPChi = nullptr;
+  cplx* SigmaV = nullptr;     // (NIBZ*Nf)
+  cplx* order2 = nullptr;     // (Nt)
+  cplx* GGG = nullptr;        // (Nx*Ng, Ny*Ng, Nf) U^2 term after the FFT
+  double* scal = nullptr;     // device scalars, see Scal
+  double* red = nullptr;      // reduction scratch
+};
+
+// slots of DeviceState::scal
+enum Scal {
+  S_MU = 0,         // chemical potential
+  S_T1 = 1,         // last particle number estimate
+  S_STEPS = 2,      // bisection steps of the last calc_Gkw_Grt
+  S_STATUS = 3,     // 0 ok, else a TUPS_ERR_* code set by a device routine
+  S_RELSIG = 4,     // conv: max relative Sigma change
+  S_RELSIGAV = 5,   // conv: |sum rel| / Nt
+  S_DSIG = 6,       // conv: max |dSigma|
+  S_FMAX = 7,       // conv: max|F_r|, 4 slots (7..10)
+  S_NANFLAG = 11,   // conv: NaN/Inf seen
+  S_COUNT = 16
+};
+
+}  // namespace tups
+
+struct tups_ctx {
+  tups_params p{};
+  tups_dims d{};
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  long long launches = 0;
+  // host tables
+  std::vector<int> pick, bonds0, signs, reps, lsym, ibz, symlist, symq;
+  std::vector<double> FF, FF_inv, lfac, Ek, Ekg;
+  double aux = 1.0;         // 1/FF(1,1,1)^2
+  // host copies of small state
+  double F_max_prev[4] = {0, 0, 0, 0};
+  bool have_exp = false, have_M = false, have_phir = false, have_green = false;
+  tups::DeviceTables t;
+  tups::DeviceState s;
+  std::vector<void*> allocations;
+};
+
+namespace tups {
+
+int set_error(tups_ctx* ctx, int code, const std::string& msg);
+int cuda_check(tups_ctx* ctx, cudaError_t e, const char* what);
+// record a kernel launch and check for launch errors
+int after_launch(tups_ctx* ctx, const char* name);
+
+// kernel drivers (each returns TUPS_OK or an error code)
+int launch_sigma_hartree(tups_ctx* ctx);
+int launch_bisection(tups_ctx* ctx, int cal_chi, int max_steps);
+int launch_grt(tups_ctx* ctx);
+int launch_gkw(tups_ctx* ctx);
+int launch_chi(tups_ctx* ctx, int q_begin, int q_count);
+int launch_bse_chunk(tups_ctx* ctx, int q_begin, int q_count);
+int launch_phir(tups_ctx* ctx);
+int launch_M(tups_ctx* ctx, int which);
+int launch_pae(tups_ctx* ctx);
+int launch_sde(tups_ctx* ctx);
+int launch_conv(tups_ctx* ctx);
+int launch_vertex_update(tups_ctx* ctx);
+int launch_output_mu(tups_ctx* ctx);
+int launch_fft2d(tups_ctx* ctx, const cplx* in, cplx* out, int forward);
+int launch_chi_aux(tups_ctx* ctx);
+
+}  // namespace tups

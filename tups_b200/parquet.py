@@ -1,0 +1,340 @@
+"""Host-side mirror of the reference's Fortran module interface.
+
+``Solver`` holds one device context.  Its methods carry the names of the
+reference routines they replace and take the same arguments:
+
+=========================  ==================================================
+reference (module :: name)  here
+=========================  ==================================================
+parquet_ini::set_parameters ``read_prms(path)``
+parquet_chi::calc_Gkw_Grt   ``Solver.calc_Gkw_Grt(ite, cal_chi)``
+parquet_chi::calc_chi       ``Solver.calc_chi(idx_q)``
+Parquet_kernel::BSE         ``Solver.BSE(ite)``
+parquet_PhiR::calc_PhiR     ``Solver.calc_PhiR(ite)`` (+ calculate_expSqR/qSR)
+parquet_EQMatrix::calc_M_*  ``Solver.calc_M_phbar_to_ph()`` etc.
+parquet_EQOuter::calculate_PAE ``Solver.calculate_PAE()``
+parquet_SDE::calc_SDE       ``Solver.calc_SDE(ite)``
+parquet_check::conv         ``Solver.conv()``
+loop::execute_loop          ``Solver.execute_loop()``
+=========================  ==================================================
+
+The module-global arrays of ``parquet_ini`` are read and written through
+properties (``Sigma``, ``F(channel)``, ``G(channel)``, ``mu`` ...) in the
+reference's Fortran layouts.  Every call goes to the CUDA library; a failing
+call raises ``TupsError``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, fields
+
+import numpy as np
+
+from . import _lib
+from ._lib import TupsError, tups_conv_info, tups_dims, tups_params
+
+CHANNELS = "dmst"
+
+
+@dataclass
+class Params:
+    """The 21 prms records (SRC/parquet_ini.f90:300-322) plus extensions."""
+    beta: float = 2.0
+    U: float = 2.0
+    nParticle: float = 1.0
+    Nx: int = 4
+    Nf: int = 16
+    neighbours: int = 1
+    readinpick: bool = False
+    pick_file: str = ""
+    Ngrain: int = 1
+    f_range: int = 0
+    f_damping: float = 0.5
+    ite_max: int = 10
+    DGA: bool = False
+    fname_L: str = ""
+    use_sig_dmft: bool = False
+    fname_sig_dmft: str = ""
+    use_U2: bool = True
+    save_F: bool = False
+    oneshot: bool = False
+    old: bool = False
+    SDE_old: bool = False
+    tprime: float = 0.0
+    conv_abs: float = 0.0
+
+    def to_c(self) -> tups_params:
+        p = tups_params()
+        for f in fields(self):
+            v = getattr(self, f.name)
+            if isinstance(v, str):
+                v = v.encode()[:255]
+            elif isinstance(v, bool):
+                v = int(v)
+            setattr(p, f.name, v)
+        return p
+
+    @classmethod
+    def from_c(cls, p: tups_params) -> "Params":
+        kw = {}
+        for f in fields(cls):
+            v = getattr(p, f.name)
+            if f.type in ("bool", bool):
+                v = bool(v)
+            elif isinstance(v, bytes):
+                v = v.decode()
+            kw[f.name] = v
+        return cls(**kw)
+
+
+def _check(lib, ctx, rc: int) -> None:
+    if rc != _lib.TUPS_OK:
+        msg = lib.tups_last_error(ctx).decode() if ctx else lib.tups_strerror(rc).decode()
+        raise TupsError(rc, msg or lib.tups_strerror(rc).decode())
+
+
+def read_prms(path: str, tprime: float = 0.0, conv_abs: float = 0.0) -> Params:
+    """``set_parameters``: parse a 21-record prms file with the native parser."""
+    lib = _lib.load()
+    p = tups_params()
+    rc = lib.tups_read_prms(str(path).encode(), C.byref(p))
+    if rc != 0:
+        raise TupsError(rc, f"cannot read prms file {path}")
+    out = Params.from_c(p)
+    out.tprime, out.conv_abs = tprime, conv_abs
+    return out
+
+
+def _ptr(a: np.ndarray) -> C.c_void_p:
+    return C.c_void_p(a.ctypes.data)
+
+
+class Solver:
+    """One parquet solver instance with device-resident state."""
+
+    def __init__(self, params: Params, device: int = 0):
+        self._lib = _lib.load()
+        self.params = params
+        self._cp = params.to_c()
+        h = C.c_void_p()
+        rc = self._lib.tups_ctx_create(C.byref(self._cp), device, C.byref(h))
+        if rc != 0:
+            raise TupsError(rc, "tups_ctx_create failed (see stderr)")
+        self._ctx = h
+        d = tups_dims()
+        self._call("tups_get_dims", C.byref(d))
+        self.dims = {f[0]: getattr(d, f[0]) for f in d._fields_}
+        for k, v in self.dims.items():
+            setattr(self, k, v)
+
+    # -- plumbing --
+    def _call(self, name: str, *args) -> None:
+        rc = getattr(self._lib, name)(self._ctx, *args)
+        _check(self._lib, self._ctx, rc)
+
+    def close(self) -> None:
+        if getattr(self, "_ctx", None):
+            self._lib.tups_ctx_destroy(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def kernel_launches(self) -> int:
+        return int(self._lib.tups_kernel_launches(self._ctx))
+
+    # -- module parquet_chi --
+    def calc_Gkw_Grt(self, ite: int, cal_chi: bool = False) -> None:
+        self._call("tups_calc_Gkw_Grt", int(ite), int(bool(cal_chi)))
+
+    def calc_chi(self, idx_q: int) -> tuple[np.ndarray, np.ndarray]:
+        """Dense (Nz, Nz) chi_ph_LL, chi_pp_LL for the 1-based slot idx_q."""
+        ph = np.zeros((self.Nz, self.Nz), dtype=np.complex128, order="F")
+        pp = np.zeros((self.Nz, self.Nz), dtype=np.complex128, order="F")
+        self._call("tups_calc_chi", int(idx_q), _ptr(ph), _ptr(pp))
+        return ph, pp
+
+    # -- module Parquet_kernel --
+    def BSE(self, ite: int = 0) -> None:
+        self._call("tups_BSE", int(ite))
+
+    # -- module parquet_PhiR --
+    def calculate_expSqR(self) -> None:
+        self._call("tups_calculate_expSqR")
+
+    def calculate_expqSR(self) -> None:
+        self._call("tups_calculate_expqSR")
+
+    def calc_PhiR(self, ite: int = 0) -> None:
+        self._call("tups_calc_PhiR", int(ite))
+
+    # -- module parquet_EQMatrix --
+    def calc_M_phbar_to_ph(self) -> None:
+        self._call("tups_calc_M_phbar_to_ph")
+
+    def calc_M_pp_to_ph(self) -> None:
+        self._call("tups_calc_M_pp_to_ph")
+
+    def calc_M_ph_to_pp(self) -> None:
+        self._call("tups_calc_M_ph_to_pp")
+
+    def calc_M_phbar_to_pp(self) -> None:
+        self._call("tups_calc_M_phbar_to_pp")
+
+    # -- module parquet_EQOuter --
+    def calculate_PAE(self) -> None:
+        self._call("tups_calculate_PAE")
+
+    # -- module parquet_SDE --
+    def calc_SDE(self, ite: int = 0) -> None:
+        self._call("tups_calc_SDE", int(ite))
+
+    # -- module parquet_check --
+    def conv(self) -> dict:
+        ci = tups_conv_info()
+        self._call("tups_conv", C.byref(ci))
+        return _conv_dict(ci)
+
+    # -- loop.f90 --
+    def vertex_update(self) -> None:
+        self._call("tups_vertex_update")
+
+    def output_block(self) -> None:
+        self._call("tups_output_block")
+
+    def iteration(self, ite: int) -> dict:
+        ci = tups_conv_info()
+        self._call("tups_iteration", int(ite), C.byref(ci))
+        return _conv_dict(ci)
+
+    def execute_loop(self) -> tuple[int, bool]:
+        ite = C.c_int(0)
+        conv = C.c_int(0)
+        self._call("tups_execute_loop", C.byref(ite), C.byref(conv))
+        return ite.value, bool(conv.value)
+
+    def synchronize(self) -> None:
+        self._call("tups_synchronize")
+
+    # -- state in reference layouts --
+    @property
+    def Sigma(self) -> np.ndarray:
+        a = np.empty(self.Nt, dtype=np.complex128)
+        self._call("tups_get_sigma", _ptr(a))
+        return a
+
+    @Sigma.setter
+    def Sigma(self, v) -> None:
+        a = np.ascontiguousarray(v, dtype=np.complex128).reshape(self.Nt)
+        self._call("tups_set_sigma", _ptr(a))
+
+    @property
+    def SigmaOld(self) -> np.ndarray:
+        a = np.empty(self.Nt, dtype=np.complex128)
+        self._call("tups_get_sigma_old", _ptr(a))
+        return a
+
+    @property
+    def Gkw(self) -> np.ndarray:
+        a = np.empty(self.Nt, dtype=np.complex128)
+        self._call("tups_get_Gkw", _ptr(a))
+        return a
+
+    @property
+    def Grt(self) -> np.ndarray:
+        n1 = self.Nx * self.Ngrain
+        a = np.empty((n1, n1, self.Nf), dtype=np.complex128, order="F")
+        self._call("tups_get_Grt", _ptr(a))
+        return a
+
+    @property
+    def mu(self) -> float:
+        v = C.c_double()
+        self._call("tups_get_mu", C.byref(v))
+        return v.value
+
+    @mu.setter
+    def mu(self, v: float) -> None:
+        self._call("tups_set_mu", C.c_double(v))
+
+    def _vertex(self, channel, which: int) -> np.ndarray:
+        ch = CHANNELS.index(channel) if isinstance(channel, str) else int(channel)
+        a = np.empty((self.Nz, self.Nz, self.Nb), dtype=np.complex128, order="F")
+        self._call("tups_get_vertex", ch, which, _ptr(a))
+        return a
+
+    def F(self, channel) -> np.ndarray:
+        """Complete vertex F_r, (Nz, Nz, Nb)."""
+        return self._vertex(channel, 0)
+
+    def G(self, channel) -> np.ndarray:
+        """G_r array: Gamma_r, or Phi_r between BSE and the vertex update."""
+        return self._vertex(channel, 1)
+
+    def set_vertex(self, channel, which: int, v: np.ndarray) -> None:
+        ch = CHANNELS.index(channel) if isinstance(channel, str) else int(channel)
+        a = np.asfortranarray(v, dtype=np.complex128)
+        self._call("tups_set_vertex", ch, which, _ptr(a))
+
+    def PhiR(self, channel) -> np.ndarray:
+        ch = CHANNELS.index(channel) if isinstance(channel, str) else int(channel)
+        a = np.empty((self.Nz * self.Nz, self.Nf // 2, self.NR), dtype=np.complex128, order="F")
+        self._call("tups_get_PhiR", ch, _ptr(a))
+        return a
+
+    def M(self, which: int) -> np.ndarray:
+        nl = self.Nl
+        a = np.empty((nl, nl, nl, nl, self.Nb, self.NR), dtype=np.complex128, order="F")
+        self._call("tups_get_M", int(which), _ptr(a))
+        return a
+
+    def expSqR(self) -> np.ndarray:
+        a = np.empty((self.NIBZ, self.NR, 8), dtype=np.complex128, order="F")
+        self._call("tups_get_expSqR", _ptr(a))
+        return a
+
+    def expqSR(self) -> np.ndarray:
+        a = np.empty((self.Nc, self.NR, 8), dtype=np.complex128, order="F")
+        self._call("tups_get_expqSR", _ptr(a))
+        return a
+
+    def tables(self) -> dict:
+        nl, nx = self.Nl, self.Nx
+        FF = np.empty((nx, nx, nl), order="F")
+        FFi = np.empty((8, nx, nx, nl), order="F")
+        signs = np.empty(nl, dtype=np.int32)
+        reps = np.empty(nl, dtype=np.int32)
+        lsym = np.empty((8, nl), dtype=np.int32, order="F")
+        lfac = np.empty((8, nl), order="F")
+        ibz = np.empty((3, self.Nred), dtype=np.int32, order="F")
+        self._call("tups_get_tables", *(_ptr(x) for x in (FF, FFi, signs, reps, lsym, lfac, ibz)))
+        return {"FF": FF, "FF_inv": FFi, "signs": signs, "reps": reps, "lsym": lsym, "lfac": lfac,
+                "ibz": ibz.T.copy()}
+
+    def sde_aux(self) -> dict:
+        na = (self.Nl * self.nbox, self.Nb)
+        nz = (self.Nz, self.Nb)
+        out = {k: np.empty(s, dtype=np.complex128, order="F") for k, s in
+               (("chi_aux_ph", na), ("chi_aux_pp", na), ("LChi", nz), ("PhChi", nz), ("PPChi", nz))}
+        self._call("tups_get_sde_aux", *(_ptr(out[k]) for k in ("chi_aux_ph", "chi_aux_pp", "LChi", "PhChi",
+                                                                "PPChi")))
+        return out
+
+
+def _conv_dict(ci: tups_conv_info) -> dict:
+    d = {"rel_sig_max": ci.rel_sig_max, "rel_sig_av": ci.rel_sig_av, "dsigma_inf": ci.dsigma_inf,
+         "mu": ci.mu, "bisection_steps": ci.bisection_steps, "converged": bool(ci.converged)}
+    for i, r in enumerate(CHANNELS):
+        d[f"F_{r}_max"] = ci.F_max[i]
+        d[f"rel_err_{r}"] = ci.rel_err[i]
+    return d
