@@ -1,0 +1,378 @@
+#!/usr/bin/env python
+"""Benchmark: seconds per parquet iteration of the TUPS loop on one B200.
+
+Workload (default): the plain PA Hubbard loop on an 8x8 k grid with 5 form
+factors and 32 fermionic / 16 bosonic Matsubara frequencies, t=1, t'=0,
+U=2, beta=5, n=1, linear mixing 0.5, complex128 storage.  A step is one
+parquet iteration (Green's function + mu bisection, BSE, Phi(R), parquet
+equation, Schwinger-Dyson, convergence check, vertex update).  The state
+(~0.9 GB) is resident in HBM and larger than L2, so no L2 flush is needed.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl {tups,reference}]
+
+Prints one JSON line (rank 0).  ``--impl reference`` times the CPU
+restatement of the reference (the reference's Fortran cannot be built in
+this image) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOADS = {
+    # name: prms fields
+    "pa_8x8_nl5_nf32": dict(beta=5.0, U=2.0, nParticle=1.0, Nx=8, Nf=32, neighbours=2, f_damping=0.5,
+                            use_U2=True, ite_max=100000),
+    "pa_4x4_nl1_nf16": dict(beta=2.0, U=2.0, nParticle=1.0, Nx=4, Nf=16, neighbours=1, f_damping=0.5,
+                            use_U2=True, ite_max=100000),
+    "pa_16x16_nl9_nf64": dict(beta=10.0, U=3.0, nParticle=0.85, Nx=16, Nf=64, neighbours=3, f_damping=0.5,
+                              use_U2=True, ite_max=100000, tprime=-0.2),
+}
+DEFAULT_WORKLOAD = "pa_8x8_nl5_nf32"
+METRIC = "s/parquet-iter"
+METRIC_FULL = "s/parquet-iter & BSE TFLOP/s: split-precision vs FP64 GPU path, Σ rel.err≤1e-10"
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except (OSError, ValueError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def fp64_peak_tflops(device: int) -> float:
+    """cuBLAS ZGEMM throughput (torch complex128 matmul, 4096^3, best of 5)."""
+    import torch
+    n = 4096
+    a = torch.randn(n, n, dtype=torch.complex128, device=f"cuda:{device}")
+    b = torch.randn(n, n, dtype=torch.complex128, device=f"cuda:{device}")
+    for _ in range(2):
+        a @ b
+    torch.cuda.synchronize(device)
+    best = math.inf
+    for _ in range(5):
+        s = torch.cuda.Event(enable_timing=True)
+        e = torch.cuda.Event(enable_timing=True)
+        s.record()
+        a @ b
+        e.record()
+        torch.cuda.synchronize(device)
+        best = min(best, s.elapsed_time(e))
+    del a, b
+    torch.cuda.empty_cache()
+    return 8.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text())
+        except ValueError:
+            pass
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "fallback": True}
+
+
+def pae_valid_count(d: dict, ibz: np.ndarray) -> int:
+    """Number of (slot, nu1, nu2, target pair, contribution type) that the
+    crossing kernel contracts (each over Nl^4 NR terms per target)."""
+    Nf = d["Nf"]
+    nh = Nf // 2
+    W = ibz[:, 2][:, None, None]
+    n1 = np.arange(1, Nf + 1)[None, :, None]
+    n2 = np.arange(1, Nf + 1)[None, None, :]
+    tot = 0
+    for ww, lo in ((n2 - n1 + 1, 1), (n1 - n2 + 1, 2), (n1 + n2 + W - Nf - 1, 1), (Nf + 3 - n1 - n2 - W, 2),
+                   (W - n1 - n2 + Nf + 1, 1), (n1 + n2 - W - Nf + 1, 2), (n2 - n1 + 1, 1), (n1 - n2 + 1, 2)):
+        ww = np.broadcast_to(ww, (len(ibz), Nf, Nf))
+        tot += int(np.count_nonzero((ww >= lo) & (ww <= nh)))
+    return tot
+
+
+def read_traffic(kernel: str, workload: str):
+    """Per-launch DRAM bytes of a kernel from the committed ncu summary
+    ``profiles/traffic.txt`` (lines: kernel workload bytes_per_launch)."""
+    p = ROOT / "profiles" / "traffic.txt"
+    if not p.exists():
+        return None
+    for ln in p.read_text().splitlines():
+        f = ln.split()
+        if len(f) >= 3 and not ln.startswith("#") and f[0] == kernel and f[1] == workload:
+            try:
+                return float(f[2])
+            except ValueError:
+                return None
+    return None
+
+
+def oracle_params(wl: dict):
+    from oracle import tups_oracle as O
+    kw = {k: v for k, v in wl.items() if k in O.Params.__dataclass_fields__}
+    return O.Params(**kw)
+
+
+def cpu_oracle_seconds_per_iteration(wl: dict, timed_iterations: int = 1, warm_iterations: int = 1):
+    """Time the oracle port: warm (untimed) iterations, then timed ones."""
+    from oracle import tups_oracle as O
+    st = O.initialize(oracle_params(wl))
+    for ite in range(warm_iterations):
+        O.iteration(st, ite)
+    t0 = time.perf_counter()
+    for ite in range(warm_iterations, warm_iterations + timed_iterations):
+        O.iteration(st, ite)
+    return (time.perf_counter() - t0) / timed_iterations
+
+
+def blas_threads() -> int:
+    try:
+        from threadpoolctl import threadpool_info
+        n = [i.get("num_threads", 1) for i in threadpool_info() if i.get("user_api") == "blas"]
+        if n:
+            return int(max(n))
+    except Exception:
+        pass
+    return os.cpu_count() or 1
+
+
+def run_reference(args, wl_name: str, wl: dict):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    steps = max(1, min(args.steps, 3))
+    warm = 1
+    spi = cpu_oracle_seconds_per_iteration(wl, timed_iterations=steps, warm_iterations=warm)
+    cores = blas_threads()
+    line = {
+        "impl": "reference", "metric": METRIC, "metric_full": METRIC_FULL, "value": spi, "unit": "s/iter",
+        "n_gpus": ws, "steps": steps, "warmup": warm, "ms_per_step": spi * 1e3, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": wl_name, **{k: wl[k] for k in ("Nx", "Nf", "neighbours", "beta", "U", "nParticle")},
+                   "parallelism": "host cores"},
+        "cpu_baseline": {"value": spi, "unit": "s/iter", "cores": cores, "kind": "port",
+                         "sample": f"{steps} oracle iteration(s) after {warm} untimed; numpy/OpenBLAS "
+                                   "restatement (the Fortran reference has no compiler in this image)"},
+        "e2e": {"value": spi, "unit": "s/iter", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_tups(args, wl_name: str, wl: dict):
+    import torch
+    ws, rank, local = dist_env()
+    device = local
+    torch.cuda.set_device(device)
+    pg = None
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+        pg = dist
+    from tups_b200 import Params, Solver, load
+    load()
+    peak64 = fp64_peak_tflops(device)
+    params = Params(**{k: v for k, v in wl.items() if k in Params.__dataclass_fields__})
+    sol = Solver(params, device=device)
+    K, W = args.steps, args.warmup
+    for ite in range(W):
+        sol.iteration(ite)
+    sol.synchronize()
+    # ---- timed region: K iterations, device-resident state ----
+    sol.set_timing(True)
+    l0 = sol.kernel_launches
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize(device)
+    sol.synchronize()
+    clocks = ClockSampler(device)
+    clocks.start()
+    sol.record_event(0)
+    infos = []
+    for k in range(K):
+        infos.append(sol.iteration(W + k))
+    sol.record_event(1)
+    ms = sol.event_elapsed_ms(0, 1)
+    sol.synchronize()
+    torch.cuda.synchronize(device)
+    clk = clocks.stop()
+    launches = sol.kernel_launches - l0
+    phases = sol.phase_times()
+    sol.set_timing(False)
+    # ---- e2e: Sigma from pinned host, one iteration, Sigma back to pinned host ----
+    nt = sol.Nt
+    h_in = torch.empty(2 * nt, dtype=torch.float64, pin_memory=True).numpy().view(np.complex128)
+    h_out = torch.empty(2 * nt, dtype=torch.float64, pin_memory=True).numpy().view(np.complex128)
+    h_in[:] = sol.Sigma
+    if pg:
+        pg.barrier()
+    sol.synchronize()
+    sol.record_event(2)
+    for k in range(K):
+        sol.set_sigma_from(h_in)
+        sol.iteration(W + K + k)
+        sol.get_sigma_into(h_out)
+        h_in[:] = h_out
+    sol.record_event(3)
+    ms_e2e = sol.event_elapsed_ms(2, 3)
+    # ---- max over ranks ----
+    if pg:
+        t = torch.tensor([ms, ms_e2e], dtype=torch.float64, device=f"cuda:{device}")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms, ms_e2e = float(t[0]), float(t[1])
+    value = ms * 1e-3 / (K * ws)
+    e2e_value = ms_e2e * 1e-3 / (K * ws)
+    d = sol.dims
+    # ---- roofline of the kernels ----
+    tab = sol.tables()
+    n_valid = pae_valid_count(d, tab["ibz"])
+    Nz, Nl, NR, Nb, nh = d["Nz"], d["Nl"], d["NR"], d["Nb"], d["Nf"] // 2
+    kern = {}
+    ms_g, c_g = phases["bse_gemm"]
+    if c_g:
+        # per launch: 16 Nz^3 for each (q, r) instance; launches split the Nb slots in chunks
+        fl = 16.0 * Nz ** 3 * 4 * Nb / (c_g / K)
+        kern["k_bse_gemm"] = {"ms": ms_g, "launches": c_g, "bound": "tensor", "unit": "TFLOP/s",
+                              "achieved": fl / (ms_g / c_g * 1e-3) / 1e12, "peak": peak64,
+                              "peak_source": "FP64 cuBLAS ZGEMM 4096^3 measured in this run"}
+    ms_p, c_p = phases["pae"]
+    if c_p:
+        fl = 8.0 * 2 * Nl ** 4 * NR * n_valid / (c_p / K)
+        kern["k_pae"] = {"ms": ms_p, "launches": c_p, "bound": "tensor", "unit": "TFLOP/s",
+                         "achieved": fl / (ms_p / c_p * 1e-3) / 1e12, "peak": peak64,
+                         "peak_source": "FP64 cuBLAS ZGEMM 4096^3 measured in this run (FP64 pipe)"}
+    ms_r, c_r = phases["phir"]
+    if c_r:
+        by = 16.0 * (4 * Nb * Nz * Nz + 4 * Nz * Nz * nh * NR)
+        pk = measured_peaks()
+        kern["k_phir"] = {"ms": ms_r, "launches": c_r, "bound": "hbm", "unit": "GB/s",
+                          "achieved": by / (ms_r / c_r * 1e-3) / 1e9, "peak": pk.get("hbm_gbs"),
+                          "peak_source": "MEASURED_PEAKS.json hbm_gbs" + (" (fallback)" if pk.get("fallback") else "")}
+    dom = max(kern, key=lambda k: kern[k]["ms"]) if kern else None
+    roof = None
+    if dom:
+        kd = kern[dom]
+        roof = {"kernel": dom, "bound": kd["bound"], "achieved": kd["achieved"], "peak": kd["peak"],
+                "unit": kd["unit"], "frac": kd["achieved"] / kd["peak"] if kd["peak"] else None,
+                "traffic": read_traffic(dom, wl_name), "peak_source": kd["peak_source"]}
+    bse_tflops = kern.get("k_bse_gemm", {}).get("achieved")
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        sec = cpu_oracle_seconds_per_iteration(wl)
+        cpu = {"value": sec, "unit": "s/iter", "cores": blas_threads(), "kind": "port",
+               "sample": "1 oracle iteration (ite 1, after an untimed ite 0) of the same workload; "
+                         "numpy/OpenBLAS restatement of the reference"}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "metric_full": METRIC_FULL, "value": value, "unit": "s/iter", "n_gpus": ws,
+            "steps": K, "warmup": W, "ms_per_step": ms / K, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": wl_name,
+                       **{k: wl[k] for k in ("Nx", "Nf", "neighbours", "beta", "U", "nParticle")},
+                       "tprime": wl.get("tprime", 0.0), "Nl": d["Nl"], "Nz": Nz, "Nred": d["Nred"], "NR": NR,
+                       "l2": "resident state ~%.2f GB > 126 MB L2; no flush" % (
+                           (8 * Nz * Nz * Nb * 16) / 1e9),
+                       "parallelism": "replicas" if ws > 1 else "single GPU"},
+            "bse_tflops": bse_tflops,
+            "roofline": roof,
+            "kernels": kern,
+            "phase_ms_per_iter": {p: v[0] / K for p, v in phases.items()},
+            "e2e": {"value": e2e_value, "unit": "s/iter", "h2d_bytes_per_step": 16 * nt,
+                    "d2h_bytes_per_step": 16 * nt + 2 * 16 * 8,
+                    "api": "Solver.set_sigma_from(pinned) + Solver.iteration + Solver.get_sigma_into(pinned)"},
+            "gpu_launches": launches,
+            "clocks": clk,
+            "cpu_baseline": cpu,
+            "last_conv": {k: infos[-1][k] for k in ("rel_sig_max", "dsigma_inf", "mu")} if infos else None,
+        }
+        print(json.dumps(line), flush=True)
+    sol.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["tups", "reference"], default="tups")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "tups":
+        args.warmup = 3
+    wl = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        run_reference(args, args.workload, wl)
+    else:
+        run_tups(args, args.workload, wl)
+
+
+if __name__ == "__main__":
+    main()

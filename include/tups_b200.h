@@ -104,6 +104,12 @@ int tups_read_prms(const char* path, tups_params* out);
  * fills device state on `device`. */
 int tups_ctx_create(const tups_params* p, int device, tups_ctx** out);
 int tups_ctx_destroy(tups_ctx* ctx);
+/* Host-only part of tups_ctx_create (no device needed): derived sizes and the
+ * form-factor / symmetry / index tables in the layouts of tups_get_tables.
+ * Lets a caller size its host arrays before creating a context. Any output
+ * pointer may be NULL. */
+int tups_host_tables(const tups_params* p, tups_dims* d, double* FF, double* FF_inv, int* signs, int* reps,
+                     int* lsym, double* lfac, int* ibz);
 int tups_get_dims(const tups_ctx* ctx, tups_dims* out);
 const char* tups_last_error(const tups_ctx* ctx);
 const char* tups_strerror(int status);
@@ -187,6 +193,29 @@ int tups_get_sde_aux(tups_ctx* ctx, double* chi_aux_ph, double* chi_aux_pp,
 int tups_synchronize(tups_ctx* ctx);
 /* number of this library's kernels launched since context creation */
 long long tups_kernel_launches(const tups_ctx* ctx);
+
+/* ---- instrumentation (the per-phase timings of SRC/loop.f90:64-178, taken
+ * with CUDA events on the library's stream) ---------------------------------- */
+#define TUPS_PHASE_GREEN 0     /* calc_Gkw_Grt */
+#define TUPS_PHASE_CHI 1       /* calc_chi (all slots) */
+#define TUPS_PHASE_BSE_PREP 2  /* Gamma chi, chi Gamma */
+#define TUPS_PHASE_BSE_GEMM 3  /* the K = 2 Nz tensor-core GEMM */
+#define TUPS_PHASE_PHIR 4      /* calc_PhiR */
+#define TUPS_PHASE_M 5         /* calc_M_* */
+#define TUPS_PHASE_PAE 6       /* calculate_PAE */
+#define TUPS_PHASE_SDE 7       /* calc_SDE */
+#define TUPS_PHASE_CONV 8      /* conv */
+#define TUPS_PHASE_UPDATE 9    /* vertex update */
+#define TUPS_NPHASE 10
+/* enable (1) / disable (0) phase timing; enabling clears the accumulators */
+int tups_set_timing(tups_ctx* ctx, int enable);
+/* milliseconds accumulated per phase since timing was enabled, and the
+ * number of timed launches of each (each array TUPS_NPHASE long; NULL ok) */
+int tups_get_phase_times(tups_ctx* ctx, double* ms, int* count);
+/* record a CUDA event on the library's stream in slot 0..7 */
+int tups_record_event(tups_ctx* ctx, int slot);
+/* milliseconds between two recorded slots (synchronizes on the later one) */
+int tups_event_elapsed(tups_ctx* ctx, int slot_a, int slot_b, double* ms);
 
 #ifdef __cplusplus
 }

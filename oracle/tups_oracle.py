@@ -989,6 +989,7 @@ def calc_M(st: State) -> None:
         M2d = np.einsum("skd,kb,krs->bdrs", FFinvk[:, qmk, :], FFk, E)
         Mphbar_pp[:, :, :, :, iq, :] = np.einsum("acrs,bdrs->abcdr", M1m, M2d)
     qi = np.arange(st.Nb) // (st.Nf // 2)
+    st.arrays.pop("_M_matrix", None)
     st.arrays["M_ibz"] = {"phbar_to_ph": Mphbar_ph, "pp_to_ph": Mpp_ph,
                           "ph_to_pp": Mph_pp, "phbar_to_pp": Mphbar_pp}
     st.arrays["M_q_of_slot"] = qi
@@ -1093,16 +1094,31 @@ def crossing_contribution(st: State, call: str, PhiR: np.ndarray, w2: int) -> tu
     l = np.arange(Nl)
     ai = np.clip(a, 1, Nf) - 1
     bi = np.clip(b, 1, Nf) - 1
-    rows = l[:, None, None, None] * Nf + ai[None, None, :, :]  # (l3,1,q,nu)
-    cols = l[None, :, None, None] * Nf + bi[None, None, :, :]  # (1,l4,q,nu)
-    X = P[rows, cols, :]  # (l3, l4, q, nu, R)
+    rows = l[None, :, None, None] * Nf + ai[:, None, None, :]  # (q,l3,1,nu)
+    cols = l[None, None, :, None] * Nf + bi[:, None, None, :]  # (q,1,l4,nu)
+    X = P[rows, cols, :]  # (q, l3, l4, nu, R)
     if tr:
         sg = st.signs.astype(np.float64)
-        X = (sg[:, None] * sg[None, :])[:, :, None, None, None] * np.conj(X)
-    X = np.where(valid[None, None, :, :, None], X, 0.0)
-    Mq = st.M_ibz[mname][:, :, :, :, st.M_q_of_slot, :]  # (l1,l2,l3,l4,q,R)
-    C = np.einsum("abcdqr,cdqnr->abqn", Mq, X, optimize=True)
+        X = (sg[:, None] * sg[None, :])[None, :, :, None, None] * np.conj(X)
+    X = np.where(valid[:, None, None, :, None], X, 0.0)
+    # contraction over (l3, l4, R) as a matmul batched over the slots of each
+    # IBZ momentum (the tensors depend on the momentum only)
+    nh = Nf // 2
+    Xm = X.transpose(0, 1, 2, 4, 3).reshape(st.NIBZ, nh, Nl * Nl * NR, Nf)
+    Mm = _M_matrix(st, mname)  # (NIBZ, 1, Nl*Nl, Nl*Nl*NR)
+    C = np.matmul(Mm, Xm)  # (NIBZ, nh, Nl*Nl, Nf)
+    C = C.reshape(st.Nb, Nl, Nl, Nf).transpose(2, 1, 0, 3)  # (l1, l2, q, nu)
     return valid, t, C
+
+
+def _M_matrix(st: State, name: str) -> np.ndarray:
+    """M_*[l1,l2,l3,l4,Q,R] as (NIBZ, 1, (l2,l1), (l3,l4,R)) for the batched matmul."""
+    cache = st.arrays.setdefault("_M_matrix", {})
+    if name not in cache:
+        M = st.M_ibz[name]  # (l1, l2, l3, l4, Q, R)
+        Nl, NR = st.Nl, st.NR
+        cache[name] = M.transpose(4, 1, 0, 2, 3, 5).reshape(st.NIBZ, 1, Nl * Nl, Nl * Nl * NR).copy()
+    return cache[name]
 
 
 def calculate_PAE(st: State) -> None:

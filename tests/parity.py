@@ -77,7 +77,11 @@ def iteration_phases(sol, st: O.State, ite: int, errs: dict) -> dict:
         cph, cpp = st.chi_aux
         lc, pc, qc = st.LChi
         errs.setdefault("chi_aux", []).append(max(rel(aux["chi_aux_ph"], cph), rel(aux["chi_aux_pp"], cpp)))
-        errs.setdefault("LChi", []).append(max(rel(aux["LChi"], lc), rel(aux["PhChi"], pc), rel(aux["PPChi"], qc)))
+        # LChi enters Sigma only as LChi + PhChi, and in the PA with the U^2
+        # term it is (L_d - L_m - 2U) chi = 0 up to rounding: scale its error
+        # by |PhChi| instead of by its own (noise-level) size
+        lchi_err = float(np.max(np.abs(aux["LChi"] - lc))) / max(float(np.max(np.abs(pc))), 1e-300)
+        errs.setdefault("LChi", []).append(max(lchi_err, rel(aux["PhChi"], pc), rel(aux["PPChi"], qc)))
         errs.setdefault("Sigma", []).append(rel(sol.Sigma, st.Sigma))
     conv_o, info_o = O.conv(st)
     info_g = sol.conv()

@@ -1,0 +1,87 @@
+"""CPU tests of the C ABI: the library loads, exports every symbol that
+include/tups_b200.h declares, and its host-side code (prms parser, index /
+symmetry / form-factor tables) agrees with the oracle without a GPU."""
+from __future__ import annotations
+
+import ctypes as C
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle import tups_oracle as O
+
+ROOT = Path(__file__).resolve().parent.parent
+GOLD = ROOT / "tests" / "golden"
+
+
+def declared_symbols() -> list[str]:
+    text = (ROOT / "include" / "tups_b200.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(tups_[a-zA-Z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol(gpu_lib):
+    names = declared_symbols()
+    assert len(names) > 40
+    for n in names:
+        assert hasattr(gpu_lib, n), n
+
+
+def test_binding_covers_header(gpu_lib):
+    from tups_b200 import exported_symbols
+    assert set(declared_symbols()) <= set(exported_symbols())
+
+
+def test_strerror(gpu_lib):
+    assert gpu_lib.tups_strerror(-3) == b"chemical potential bisection did not converge"
+    assert gpu_lib.tups_strerror(0) == b"ok"
+
+
+@pytest.mark.parametrize("name", ["pa_4x4_nl1", "pa_4x4_nl5"])
+def test_native_prms_parser(gpu_lib, name):
+    from tups_b200 import read_prms
+    p = read_prms(str(GOLD / f"prms_{name}"))
+    o = O.read_prms(str(GOLD / f"prms_{name}"))
+    for k in ("beta", "U", "nParticle", "Nx", "Nf", "neighbours", "Ngrain", "f_range", "f_damping", "ite_max",
+              "use_U2", "oneshot", "old", "SDE_old", "DGA", "pick_file"):
+        assert getattr(p, k) == getattr(o, k), k
+
+
+def test_native_prms_parser_rejects_short_file(gpu_lib, tmp_path):
+    from tups_b200 import TupsError, read_prms
+    f = tmp_path / "prms"
+    f.write_text("5.0d0\n2.0d0\n")
+    with pytest.raises(TupsError):
+        read_prms(str(f))
+
+
+@pytest.mark.parametrize("nx,nf,nb", [(4, 16, 1), (4, 8, 2), (8, 32, 2), (8, 16, 3), (16, 64, 3), (16, 8, 4)])
+def test_host_tables_bit_exact(gpu_lib, nx, nf, nb):
+    """Integer tables equal; form factors equal to the last bit (same libm)."""
+    from tups_b200 import Params
+    from tups_b200.parquet import host_tables
+    t = host_tables(Params(Nx=nx, Nf=nf, neighbours=nb))
+    st = O.initialize(O.Params(Nx=nx, Nf=nf, neighbours=nb))
+    d = t["dims"]
+    for k in ("Nl", "Nz", "Nred", "NIBZ", "NR", "Nt"):
+        assert d[k] == getattr(st, k), k
+    assert np.array_equal(t["signs"], st.signs)
+    assert np.array_equal(t["reps"], st.reps)
+    assert np.array_equal(t["lsym"], st.lsym)
+    assert np.array_equal(t["lfac"], st.lfac)
+    assert np.array_equal(t["ibz"], st.ibz)
+    assert np.array_equal(t["FF"], st.FF)
+    assert np.array_equal(t["FF_inv"], st.FF_inv)
+
+
+def test_host_tables_reject_bad_sizes(gpu_lib):
+    from tups_b200 import Params, TupsError
+    from tups_b200.parquet import host_tables
+    with pytest.raises(TupsError):
+        host_tables(Params(Nx=5, Nf=16))
+    with pytest.raises(TupsError):
+        host_tables(Params(Nx=4, Nf=15))
+    with pytest.raises(TupsError):
+        host_tables(Params(Nx=4, Nf=16, old=True))

@@ -1,0 +1,197 @@
+"""CPU tests of the oracle: the reference's own known-answer checks, physics
+invariants, loop-by-loop cross-checks and the golden fixtures."""
+from __future__ import annotations
+
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle import loops as L
+from oracle import tups_oracle as O
+
+GOLD = Path(__file__).resolve().parent / "golden"
+
+
+def small(nx=4, nf=8, nb=2, **kw):
+    return O.Params(beta=2.0, U=2.0, nParticle=0.9, Nx=nx, Nf=nf, neighbours=nb, f_damping=0.5, ite_max=10, **kw)
+
+
+@pytest.mark.parametrize("nx,nb,nl", [(4, 1, 1), (4, 2, 5), (8, 2, 5), (8, 3, 9), (16, 3, 9), (16, 4, 13)])
+def test_form_factor_known_answers(nx, nb, nl):
+    """FF_sdwave_check (parquet_check.f90:264-292) to 1e-12 and the
+    orthonormality of check_ortho (parquet_util.f90:693-725)."""
+    st = O.initialize(O.Params(Nx=nx, Nf=8, neighbours=nb))
+    assert st.Nl == nl
+    assert O.ff_sdwave_check(st.FF, nx) < 1e-12
+    orth = np.einsum("xya,xyb->ab", st.FF, st.FF)
+    assert np.abs(orth - np.eye(nl)).max() < 1e-13
+
+
+def test_bond_tables_by_reading():
+    """signs/reps of initialize_bonds (parquet_formfactors.f90:95-360) worked
+    out by hand for 9 form factors: origin; (1,0) with characters 1,3,5 and
+    its 2D partner; (1,1) with characters 1,4,5 and its partner."""
+    st = O.initialize(O.Params(Nx=8, Nf=8, neighbours=3))
+    assert st.signs.tolist() == [1, 1, 1, -1, -1, 1, 1, -1, -1]
+    assert st.reps.tolist() == [1, 1, 3, 5, 6, 1, 4, 5, 6]
+    assert st.bonds0.tolist() == [[0, 0, 1], [1, 0, 1], [1, 0, 3], [1, 0, 5], [0, 1, 5],
+                                  [1, 1, 1], [1, 1, 4], [1, 1, 5], [-1, 1, 5]]
+
+
+@pytest.mark.parametrize("nx,nb", [(4, 2), (8, 3), (16, 3)])
+def test_lspace_symmetry_matches_kspace(nx, nb):
+    """sym_op_L (parquet_util.f90:732-890) is the l-space image of the
+    k-space operation: FF(S k, l) = fac(S, l) FF(k, lsym(S, l)).
+
+    Holds for up to 9 form factors.  With 13 (neighbours = 4) the table's
+    `l_in > 5` branch, written for the diagonal (1,1) bonds, is also applied
+    to the 2D pair of the (2,0) shell and the relation breaks there; the
+    oracle and the CUDA code keep the table as the reference has it."""
+    st = O.initialize(O.Params(Nx=nx, Nf=8, neighbours=nb))
+    for s in range(1, 9):
+        for kx in range(1, nx + 1):
+            for ky in range(1, nx + 1):
+                sx, sy = O.symmetry_operation(s, kx, ky, nx)
+                lhs = st.FF[sx - 1, sy - 1, :]
+                rhs = st.lfac[s - 1] * st.FF[kx - 1, ky - 1, st.lsym[s - 1] - 1]
+                assert np.allclose(lhs, rhs, atol=1e-14)
+
+
+@pytest.mark.parametrize("nx", [4, 8, 16])
+def test_star_partition(nx):
+    """list_symmetries + symmetry_operation visit every BZ point exactly once
+    (symmetrize_array relies on it, parquet_util.f90:1215-1272)."""
+    st = O.initialize(O.Params(Nx=nx, Nf=8, neighbours=1))
+    ones = np.ones(st.NIBZ * 2, dtype=np.complex128)
+    out = O.symmetrize_array(st, 2, ones)
+    assert np.all(out == 1.0)
+
+
+def test_crossing_calls_match_loops():
+    """Vectorised crossing contributions vs a statement-by-statement
+    transliteration of parquet_EQContribs.f90:44-524 (Nl = 5, Nf = 6)."""
+    st = O.initialize(small(nf=6))
+    O.iteration(st, 0)
+    O.calc_Gkw_Grt(st, 1, False)
+    O.bse(st)
+    O.calc_PhiR(st)
+    G = {r: st.G[r].copy() for r in "dmst"}
+    O.calculate_PAE(st)
+    F = {r: G[r].copy() for r in "dmst"}
+    aux = abs(1.0 / st.FF[0, 0, 0] * 1.0 / st.FF[0, 0, 0])
+    q0 = st.ibz[:, 2] - 1
+    for r in "dmst":
+        F[r][:st.Nf, :st.Nf, :] += st.L[r][:, :, q0] * aux
+    for src in "dmst":
+        for w2 in range(1, st.Nf // 2 + 1):
+            for base, f1, f2 in O.DISPATCH[src]:
+                for call in [base] + ([base + "_TR"] if w2 > 1 else []):
+                    pair = O.CALLS[call][1]
+                    L.crossing_call_loops(st, call, st.PhiR[src], w2, f1, f2, F[pair[0]], F[pair[1]])
+    for r in "dmst":
+        assert np.abs(F[r] - st.F[r]).max() <= 1e-13 * np.abs(F[r]).max()
+
+
+def test_sde_and_symop_match_loops():
+    st = O.initialize(small(nf=6))
+    O.iteration(st, 0)
+    O.calc_Gkw_Grt(st, 1, False)
+    O.bse(st)
+    O.calc_PhiR(st)
+    O.calculate_PAE(st)
+    cph, cpp = O.calc_chi_aux(st)
+    lc, pc, qc = O.calc_chi_contractions(st, cph, cpp)
+    a = O.sde_sigma_ibz(st, lc, pc, qc)
+    b = L.sde_sigma_loops(st, lc, pc, qc)
+    assert np.abs(a - b).max() <= 1e-13 * np.abs(b).max()
+    PhiQ = st.G["d"].reshape(st.Nz * st.Nz, st.Nf // 2, st.NIBZ, order="F")
+    for s in range(1, 9):
+        src, fac = O.symop_perm(st, s)
+        assert np.array_equal(fac[:, None] * PhiQ[src, 1, :], L.symop_arr_loops(st, PhiQ, s, 2)[:, 1, :])
+
+
+def test_zero_interaction():
+    """U = 0 at half filling: every vertex and the self-energy stay zero.
+    (Off half filling the reference's bisection bracket [mu-U, mu+U]
+    collapses and its loop never ends; see test_bisection_cap.)"""
+    p = small(nb=2)
+    p.U = 0.0
+    p.nParticle = 1.0
+    st = O.initialize(p)
+    for ite in range(2):
+        O.iteration(st, ite)
+    assert np.abs(st.Sigma).max() == 0.0
+    for r in "dmst":
+        assert np.abs(st.F[r]).max() == 0.0
+
+
+def test_second_order_first_iteration():
+    """First iteration from Phi = 0 with use_U2: Sigma is the U^2 diagram of
+    calc_order_2nd plus the Lambda contributions; the Lambda-only part
+    vanishes when LChi is removed, so Sigma - order2 is linear in U^2 terms
+    of the bubble and the full Sigma scales as U^2 for small U."""
+    vals = []
+    for U in (1e-3, 2e-3):
+        p = small(nb=1, nx=4, nf=8)
+        p.U = U
+        p.nParticle = 1.0
+        st = O.initialize(p)
+        O.iteration(st, 0)
+        vals.append(st.Sigma.copy())
+    ratio = np.abs(vals[1]).max() / np.abs(vals[0]).max()
+    assert abs(ratio - 4.0) < 1e-2
+
+
+def test_self_energy_point_group_symmetry():
+    """Sigma(S k, nu) = Sigma(k, nu) for all eight operations."""
+    st = O.initialize(small(nb=2, nx=8))
+    O.iteration(st, 0)
+    S = st.Sigma.reshape(st.Nx, st.Ny, st.Nf)
+    for s in range(1, 9):
+        for kx in range(1, st.Nx + 1):
+            for ky in range(1, st.Ny + 1):
+                sx, sy = O.symmetry_operation(s, kx, ky, st.Nx)
+                assert np.allclose(S[sx - 1, sy - 1], S[kx - 1, ky - 1], rtol=1e-12, atol=1e-15)
+
+
+@pytest.mark.parametrize("name", ["pa_4x4_nl1", "pa_4x4_nl5"])
+def test_oracle_reproduces_golden(name):
+    """Regression pin of the oracle against its committed fixtures."""
+    g = np.load(GOLD / f"golden_{name}.npz")
+    p = O.read_prms(str(GOLD / f"prms_{name}"))
+    st = O.initialize(p)
+    for k in ("FF", "FF_inv", "lfac"):
+        assert np.array_equal(getattr(st, k), g[k]), k
+    for k in ("signs", "reps", "lsym", "ibz"):
+        assert np.array_equal(getattr(st, k), g[k]), k
+    for ite in range(min(3, p.ite_max)):
+        O.iteration(st, ite)
+        assert np.abs(st.Sigma - g["traj_Sigma"][ite]).max() <= 1e-13 * np.abs(g["traj_Sigma"][ite]).max()
+        assert st.mu == pytest.approx(float(g["traj_mu"][ite]), abs=1e-15)
+
+
+def test_read_prms_fortran_list_directed(tmp_path):
+    f = tmp_path / "prms"
+    f.write_text((GOLD / "prms_pa_4x4_nl5").read_text())
+    p = O.read_prms(str(f))
+    assert (p.beta, p.U, p.nParticle, p.Nx, p.Nf, p.neighbours) == (2.0, 2.0, 0.9, 4, 8, 2)
+    assert p.pick_file == "inidata/none" and p.use_U2 and not p.DGA and p.f_damping == 0.5
+
+
+def test_bisection_cap():
+    """U = 0 with n != 1: the bracket has zero width, so the unbounded
+    reference loop (parquet_chi.f90:120) would spin forever; capped here."""
+    p = small(nb=1)
+    p.U = 0.0
+    st = O.initialize(p)
+    with pytest.raises(RuntimeError, match="bisection"):
+        O.calc_Gkw_Grt(st, 0, False, max_steps=50)
+
+
+def test_mu_bisection_moves_off_half_filling():
+    st = O.initialize(small(nb=1))
+    steps = O.calc_Gkw_Grt(st, 0, False)
+    assert steps > 3
+    n = -2.0 * st.Grt[0, 0, st.Nf - 1].real
+    assert abs(n - 0.9) <= O.MU_TOL

@@ -56,6 +56,7 @@ _PROTOS = {
     "tups_read_prms": [C.c_char_p, C.POINTER(tups_params)],
     "tups_ctx_create": [C.POINTER(tups_params), C.c_int, C.POINTER(C.c_void_p)],
     "tups_ctx_destroy": [C.c_void_p],
+    "tups_host_tables": [C.POINTER(tups_params), C.POINTER(tups_dims)] + [C.c_void_p] * 7,
     "tups_get_dims": [C.c_void_p, C.POINTER(tups_dims)],
     "tups_calc_Gkw_Grt": [C.c_void_p, C.c_int, C.c_int],
     "tups_calc_chi": [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p],
@@ -90,7 +91,13 @@ _PROTOS = {
     "tups_get_tables": [C.c_void_p] + [C.c_void_p] * 7,
     "tups_get_sde_aux": [C.c_void_p] + [C.c_void_p] * 5,
     "tups_synchronize": [C.c_void_p],
+    "tups_set_timing": [C.c_void_p, C.c_int],
+    "tups_get_phase_times": [C.c_void_p, C.c_void_p, C.c_void_p],
+    "tups_record_event": [C.c_void_p, C.c_int],
+    "tups_event_elapsed": [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double)],
 }
+
+PHASES = ["green", "chi", "bse_prep", "bse_gemm", "phir", "M", "pae", "sde", "conv", "update"]
 _SPECIAL = {
     "tups_last_error": ([C.c_void_p], C.c_char_p),
     "tups_strerror": ([C.c_int], C.c_char_p),

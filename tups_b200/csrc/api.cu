@@ -56,10 +56,12 @@ int copy_h2d(tups_ctx* ctx, void* dev, const void* host, size_t bytes) {
 }
 
 int green_async(tups_ctx* ctx, int cal_chi) {
+  tups::phase_begin(ctx, TUPS_PHASE_GREEN);
   TRY(tups::launch_sigma_hartree(ctx));
   TRY(tups::launch_bisection(ctx, cal_chi, kMuMaxSteps));
   TRY(tups::launch_grt(ctx));
   TRY(tups::launch_gkw(ctx));
+  tups::phase_end(ctx, TUPS_PHASE_GREEN);
   ctx->have_green = true;
   return TUPS_OK;
 }
@@ -70,7 +72,9 @@ int bse_async(tups_ctx* ctx) {
   const int chunk_q = (int)std::max<size_t>(1, ctx->s.bse_chunk / 4);
   for (int q0 = 0; q0 < Nb; q0 += chunk_q) {
     const int nq = std::min(chunk_q, Nb - q0);
+    tups::phase_begin(ctx, TUPS_PHASE_CHI);
     TRY(tups::launch_chi(ctx, q0, nq));
+    tups::phase_end(ctx, TUPS_PHASE_CHI);
     TRY(tups::launch_bse_chunk(ctx, q0, nq));
   }
   return TUPS_OK;
@@ -82,7 +86,10 @@ int sde_async(tups_ctx* ctx) {
   TRY(tups::cuda_check(ctx,
                        cudaMemcpyAsync(ctx->s.SigmaOld, ctx->s.Sigma, bytes, cudaMemcpyDeviceToDevice, ctx->stream),
                        "SigmaOld = Sigma"));
-  return tups::launch_sde(ctx);
+  tups::phase_begin(ctx, TUPS_PHASE_SDE);
+  TRY(tups::launch_sde(ctx));
+  tups::phase_end(ctx, TUPS_PHASE_SDE);
+  return TUPS_OK;
 }
 
 }  // namespace
@@ -137,7 +144,9 @@ extern "C" int tups_calc_PhiR(tups_ctx* ctx, int ite) {
   if (!ctx) return TUPS_ERR_BADARG;
   if (!ctx->have_exp) return tups::set_error(ctx, TUPS_ERR_STATE, "calc_PhiR before calculate_expSqR");
   TRY(set_dev(ctx));
+  tups::phase_begin(ctx, TUPS_PHASE_PHIR);
   TRY(tups::launch_phir(ctx));
+  tups::phase_end(ctx, TUPS_PHASE_PHIR);
   ctx->have_phir = true;
   return tups::cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "calc_PhiR");
 }
@@ -145,7 +154,9 @@ extern "C" int tups_calc_PhiR(tups_ctx* ctx, int ite) {
 static int calc_M(tups_ctx* ctx, int which) {
   if (!ctx) return TUPS_ERR_BADARG;
   TRY(set_dev(ctx));
+  tups::phase_begin(ctx, TUPS_PHASE_M);
   TRY(tups::launch_M(ctx, which));
+  tups::phase_end(ctx, TUPS_PHASE_M);
   ctx->have_M = true;
   return TUPS_OK;
 }
@@ -159,7 +170,9 @@ extern "C" int tups_calculate_PAE(tups_ctx* ctx) {
   if (!ctx->have_M || !ctx->have_phir)
     return tups::set_error(ctx, TUPS_ERR_STATE, "calculate_PAE before calc_PhiR / calc_M_*");
   TRY(set_dev(ctx));
+  tups::phase_begin(ctx, TUPS_PHASE_PAE);
   TRY(tups::launch_pae(ctx));
+  tups::phase_end(ctx, TUPS_PHASE_PAE);
   return tups::cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "calculate_PAE");
 }
 
@@ -174,7 +187,9 @@ extern "C" int tups_calc_SDE(tups_ctx* ctx, int ite) {
 extern "C" int tups_conv(tups_ctx* ctx, tups_conv_info* info) {
   if (!ctx) return TUPS_ERR_BADARG;
   TRY(set_dev(ctx));
+  tups::phase_begin(ctx, TUPS_PHASE_CONV);
   TRY(tups::launch_conv(ctx));
+  tups::phase_end(ctx, TUPS_PHASE_CONV);
   double sc[tups::S_COUNT];
   TRY(read_scalars(ctx, sc));
   tups_conv_info ci;
@@ -209,7 +224,9 @@ extern "C" int tups_conv(tups_ctx* ctx, tups_conv_info* info) {
 extern "C" int tups_vertex_update(tups_ctx* ctx) {
   if (!ctx) return TUPS_ERR_BADARG;
   TRY(set_dev(ctx));
+  tups::phase_begin(ctx, TUPS_PHASE_UPDATE);
   TRY(tups::launch_vertex_update(ctx));
+  tups::phase_end(ctx, TUPS_PHASE_UPDATE);
   return tups::cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "vertex update");
 }
 
@@ -229,11 +246,15 @@ extern "C" int tups_iteration(tups_ctx* ctx, int ite, tups_conv_info* info) {
     TRY(tups_calculate_expSqR(ctx));
     TRY(tups_calculate_expqSR(ctx));
   }
+  tups::phase_begin(ctx, TUPS_PHASE_PHIR);
   TRY(tups::launch_phir(ctx));
+  tups::phase_end(ctx, TUPS_PHASE_PHIR);
   ctx->have_phir = true;
   if (ite == 0 || !ctx->have_M)
     for (int w = 0; w < 4; w++) TRY(calc_M(ctx, w));
+  tups::phase_begin(ctx, TUPS_PHASE_PAE);
   TRY(tups::launch_pae(ctx));
+  tups::phase_end(ctx, TUPS_PHASE_PAE);
   if (!ctx->p.oneshot || ite == ctx->p.ite_max - 1) TRY(sde_async(ctx));
   TRY(device_status(ctx));
   tups_conv_info ci;
@@ -241,7 +262,9 @@ extern "C" int tups_iteration(tups_ctx* ctx, int ite, tups_conv_info* info) {
   if (info) *info = ci;
   if (rc) return rc;
   if (ite % 5 == 0 || ite == ctx->p.ite_max - 1 || ci.converged) TRY(tups::launch_output_mu(ctx));
+  tups::phase_begin(ctx, TUPS_PHASE_UPDATE);
   TRY(tups::launch_vertex_update(ctx));
+  tups::phase_end(ctx, TUPS_PHASE_UPDATE);
   return TUPS_OK;
 }
 

@@ -233,14 +233,19 @@ int launch_bse_chunk(tups_ctx* ctx, int q_begin, int q_count) {
   }
   const size_t n2 = (size_t)d.Nz * d.Nz;
   dim3 pgrid((unsigned)std::min<size_t>(cdiv(n2, 256), 4096), 4 * q_count);
+  phase_begin(ctx, TUPS_PHASE_BSE_PREP);
   k_bse_prep<<<pgrid, 256, 0, ctx->stream>>>(P, ctx->s.chi_ph, ctx->s.chi_pp, ctx->s.bse_A, ctx->s.bse_B, q_begin,
                                              d.Nz, d.Nf, d.Nl);
   int rc = after_launch(ctx, "k_bse_prep");
+  phase_end(ctx, TUPS_PHASE_BSE_PREP);
   if (rc) return rc;
+  phase_begin(ctx, TUPS_PHASE_BSE_GEMM);
   // tile choice: 64x64 when Nz is a multiple of 64 (or large), else 32x32
-  if (d.Nz % 64 == 0 || d.Nz > 512) return run_gemm<64, 64, 16, 2, 2, 3>(ctx, P, q_begin, q_count);
-  if (d.Nz >= 32) return run_gemm<32, 32, 16, 2, 2, 3>(ctx, P, q_begin, q_count);
-  return run_gemm<16, 16, 16, 1, 2, 3>(ctx, P, q_begin, q_count);
+  if (d.Nz % 64 == 0 || d.Nz > 512) rc = run_gemm<64, 64, 16, 2, 2, 3>(ctx, P, q_begin, q_count);
+  else if (d.Nz >= 32) rc = run_gemm<32, 32, 16, 2, 2, 3>(ctx, P, q_begin, q_count);
+  else rc = run_gemm<16, 16, 16, 1, 2, 3>(ctx, P, q_begin, q_count);
+  phase_end(ctx, TUPS_PHASE_BSE_GEMM);
+  return rc;
 }
 
 }  // namespace tups

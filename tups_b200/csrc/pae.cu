@@ -2,202 +2,329 @@
 // eight crossing contributions of SRC/parquet_EQContribs.f90:44-524.
 //
 // The reference loops over source channel and w2 and scatter-adds every
-// contribution into F.  Here the loop is turned around (output-stationary):
-// for a target element F_a/F_b[(l1,nu1),(l2,nu2), q] each contribution type
-// hits it for at most ONE w2, obtained by inverting the type's frequency map,
-//   phbar_to_ph     w2 = nu2 - nu1 + 1          (F_d, F_m  <- Phi_d, Phi_m)
-//   phbar_to_ph_TR  w2 = nu1 - nu2 + 1 (>1)
-//   pp_to_ph        w2 = nu1 + nu2 + W - Nf - 1 (F_d, F_m  <- Phi_s, Phi_t)
-//   pp_to_ph_TR     w2 = Nf + 3 - nu1 - nu2 - W (>1)
-//   ph_to_pp        w2 = W - nu1 - nu2 + Nf + 1 (F_s, F_t  <- Phi_d, Phi_m)
-//   ph_to_pp_TR     w2 = nu1 + nu2 - W - Nf + 1 (>1)
-//   phbar_to_pp     w2 = nu2 - nu1 + 1          (F_s, F_t  <- Phi_d, Phi_m)
-//   phbar_to_pp_TR  w2 = nu1 - nu2 + 1 (>1)
-// (W = bosonic index of q, 1-based frequencies, w2 in 1..Nf/2).  So every F
-// element is formed once, in registers, as Phi + Lambda*Nc + sum of <= 4
-// contractions over (R, l3, l4), and written once: no atomics, deterministic.
-// The two sources of a type are combined with the dispatch factors of
-// SRC/parquet_EQOuter.f90:84-113 before the contraction.
+// contribution into F.  Here the loop is turned around (output-stationary).
+// For a target element F_a/F_b[(l1,nu1),(l2,nu2), q] (W = bosonic index of q,
+// 1-based frequencies, d = nu2 - nu1, s = nu1 + nu2, nh = Nf/2) the eight
+// calls group into two families per target pair, and inside a family at
+// most ONE (call, w2) reaches the element:
+//
+//  pair (F_d, F_m):
+//   D  phbar_to_ph     w2 = d + 1 >= 1,        Phi_R[(l3,nu1),(l4,pick(nu1+W-1))]
+//      phbar_to_ph_TR  w2 = 1 - d >= 2,        conj Phi_R[(l3,mF(nu1)),(l4,pick(Nf+2-nu1-W))]
+//   A  pp_to_ph        w2 = s + W - Nf - 1 >= 1, Phi_R[(l3,nu1),(l4,nu2)]
+//      pp_to_ph_TR     w2 = Nf + 3 - s - W >= 2, conj Phi_R[(l3,mF(nu1)),(l4,mF(nu2))]
+//  pair (F_s, F_t):
+//   A  ph_to_pp        w2 = W + Nf + 1 - s >= 1, Phi_R[(l3,nu1),(l4,nu2)]
+//      ph_to_pp_TR     w2 = s - W - Nf + 1 >= 2, conj Phi_R[(l3,mF(nu1)),(l4,mF(nu2))]
+//   D  phbar_to_pp     w2 = d + 1 >= 1,        Phi_R[(l3,nu1),(l4,pick(W+Nf-nu2))]
+//      phbar_to_pp_TR  w2 = 1 - d >= 2,        conj Phi_R[(l3,mF(nu1)),(l4,pick(nu2-W+1))]
+//
+// (w2 <= nh always; mF(x) = Nf+1-x; pick = clamp to [1, Nf]; TR terms carry
+// signs(l3) signs(l4)).  Both calls of a family use the same crossing tensor
+// M and the same two source channels, combined with the dispatch factors of
+// SRC/parquet_EQOuter.f90:84-113 as they are gathered.  So per (q, pair) the
+// whole parquet equation is ONE complex GEMM
+//     C^T[(target, element), (l1,l2)] = X^T[(target, element), (family,l3,l4,R)] M^T
+// run on the FP64 tensor cores (mma.sync m16n8k8), with X gathered from
+// Phi(R) on load and F = Phi + Lambda*Nc + C/Nx written once in the epilogue:
+// no atomics, deterministic.
 #include "tups_device.cuh"
 
 namespace tups {
 
-constexpr int PAE_NLMAX = 13;
-
 struct PaePtrs {
   const cplx* Phi[4];   // Phi_r (G arrays after the BSE), (Nz, Nz, Nb)
   const cplx* PhiR[4];  // (Nz*Nz, Nf/2, NR)
-  const cplx* M[4];     // (Nl^4, NIBZ, NR)
+  const cplx* M[4];     // (Nl^4, NIBZ, NR): 0 phbar_to_ph 1 pp_to_ph 2 ph_to_pp 3 phbar_to_pp
   const cplx* L[4];     // (Nf, Nf, Nf/2)
   cplx* F[4];
 };
 
-__device__ __forceinline__ int clampnu(int x, int Nf) { return x < 1 ? 1 : (x > Nf ? Nf : x); }
+__host__ __device__ __forceinline__ int clampnu(int x, int Nf) { return x < 1 ? 1 : (x > Nf ? Nf : x); }
 
-// Frequency map of contribution type t of target pair `pair` for the target
-// (nu1, nu2) at bosonic index W.  Returns false when the type does not reach
-// this element; otherwise w2 and the source (row, column) frequencies a, b.
-__device__ __forceinline__ bool pae_map(int pair, int t, int nu1, int nu2, int W, int Nf, int* w2, int* a, int* b) {
+// Frequency map of family fam (0 = D, 1 = A) of target pair `pair` at the
+// element (nu1, nu2).  Returns false when the family does not reach it.
+__host__ __device__ __forceinline__ bool pae_family(int pair, int fam, int nu1, int nu2, int W, int Nf, int* w2,
+                                                    int* a, int* b, int* tr) {
   const int nh = Nf / 2;
+  const int d = nu2 - nu1, s = nu1 + nu2;
   int ww;
-  if (pair == 0) {
-    switch (t) {
-      case 0:  // phbar_to_ph: nu2 = nu1 + w2 - 1, Phi_R[(l3,nu1),(l4,pick(nu1+W-1))]
-        ww = nu2 - nu1 + 1;
-        if (ww < 1 || ww > nh) return false;
-        *a = nu1;
-        *b = clampnu(nu1 + W - 1, Nf);
-        break;
-      case 1:  // phbar_to_ph_TR: nu2 = nu1 - w2 + 1, conj Phi_R[(l3,mF(nu1)),(l4,pick(mF(nu1+W-1)))]
-        ww = nu1 - nu2 + 1;
-        if (ww < 2 || ww > nh) return false;
-        *a = Nf + 1 - nu1;
-        *b = clampnu(Nf + 2 - nu1 - W, Nf);
-        break;
-      case 2:  // pp_to_ph: nu2 = BmBmF(w2, W, nu1), Phi_R[(l3,nu1),(l4,nu2)]
-        ww = nu1 + nu2 + W - Nf - 1;
-        if (ww < 1 || ww > nh) return false;
-        *a = nu1;
-        *b = nu2;
-        break;
-      default:  // pp_to_ph_TR: nu2 = mF(nu1+W+w2-2), conj Phi_R[(l3,mF(nu1)),(l4,mF(nu2))]
-        ww = Nf + 3 - nu1 - nu2 - W;
-        if (ww < 2 || ww > nh) return false;
-        *a = Nf + 1 - nu1;
-        *b = Nf + 1 - nu2;
-        break;
+  if (fam == 0) {  // diagonal families: phbar_to_ph (pair 0) / phbar_to_pp (pair 1)
+    if (d >= 0) {
+      ww = d + 1;
+      if (ww > nh) return false;
+      *tr = 0;
+      *a = nu1;
+      *b = pair == 0 ? clampnu(nu1 + W - 1, Nf) : clampnu((W - 1) - (nu1 + ww - 1) + Nf + 1, Nf);
+    } else {
+      ww = 1 - d;
+      if (ww > nh) return false;
+      *tr = 1;
+      *a = Nf + 1 - nu1;
+      *b = pair == 0 ? clampnu(Nf + 2 - nu1 - W, Nf) : clampnu(nu1 - (W + ww - 1) + 1, Nf);
     }
-  } else {
-    switch (t) {
-      case 0:  // ph_to_pp: nu2 = BmBmF(W, w2, nu1), Phi_R[(l3,nu1),(l4,nu2)]
-        ww = W - nu1 - nu2 + Nf + 1;
-        if (ww < 1 || ww > nh) return false;
-        *a = nu1;
-        *b = nu2;
-        break;
-      case 1:  // ph_to_pp_TR: nu2 = BpBmF(W, w2, nu1), conj Phi_R[(l3,mF(nu1)),(l4,FmB(nu1,W+w2-1))]
-        ww = nu1 + nu2 - W - Nf + 1;
-        if (ww < 2 || ww > nh) return false;
-        *a = Nf + 1 - nu1;
-        *b = nu1 - (W + ww - 1) + 1;
-        break;
-      case 2:  // phbar_to_pp: nu2 = nu1 + w2 - 1, Phi_R[(l3,nu1),(l4,pick(BmBmF(W,w2,nu1)))]
-        ww = nu2 - nu1 + 1;
-        if (ww < 1 || ww > nh) return false;
-        *a = nu1;
-        *b = clampnu((W - 1) - (nu1 + ww - 1) + Nf + 1, Nf);
-        break;
-      default:  // phbar_to_pp_TR: nu2 = nu1 - w2 + 1, conj Phi_R[(l3,mF(nu1)),(l4,pick(FmB(nu1,W+w2-1)))]
-        ww = nu1 - nu2 + 1;
-        if (ww < 2 || ww > nh) return false;
-        *a = Nf + 1 - nu1;
-        *b = clampnu(nu1 - (W + ww - 1) + 1, Nf);
-        break;
+  } else if (pair == 0) {  // pp_to_ph
+    ww = s + W - Nf - 1;
+    if (ww >= 1) {
+      if (ww > nh) return false;
+      *tr = 0;
+      *a = nu1;
+      *b = nu2;
+    } else {
+      ww = Nf + 3 - s - W;
+      if (ww < 2 || ww > nh) return false;
+      *tr = 1;
+      *a = Nf + 1 - nu1;
+      *b = Nf + 1 - nu2;
+    }
+  } else {  // ph_to_pp
+    ww = W + Nf + 1 - s;
+    if (ww >= 1) {
+      if (ww > nh) return false;
+      *tr = 0;
+      *a = nu1;
+      *b = nu2;
+    } else {
+      ww = s - W - Nf + 1;
+      if (ww < 2 || ww > nh) return false;
+      *tr = 1;
+      *a = Nf + 1 - nu1;
+      *b = nu1 - (W + ww - 1) + 1;
     }
   }
   *w2 = ww;
   return true;
 }
 
-// One CTA per (q slot, target pair, l1); threads over the (nu1, nu2) plane;
-// each thread keeps F_a, F_b for all l2 of its element in registers.
-__global__ void __launch_bounds__(256) k_pae(PaePtrs P, const int* __restrict__ ibz, const int* __restrict__ signs,
-                                             int Nz, int Nf, int Nl, int NIBZ, int NR, double aux, double inv_nx) {
-  const int q = blockIdx.x;
-  const int pair = blockIdx.y;
-  const int l1 = blockIdx.z;
+__device__ __forceinline__ unsigned smem_u32p(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void cp_async16p(void* sdst, const void* gsrc, bool valid) {
+  unsigned sz = valid ? 16u : 0u;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32p(sdst)), "l"(gsrc), "r"(sz));
+}
+__device__ __forceinline__ void dmma_16x8x8(double* c, const double* a, const double* b) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
+}
+
+constexpr int PAE_E = 32;          // elements per CTA
+constexpr int PAE_ROWS = 2 * PAE_E;  // (target, element) rows
+constexpr int PAE_BK = 16;
+constexpr int PAE_LDA = PAE_ROWS + 2;
+constexpr int PAE_LDB = PAE_BK + 4;
+
+// One CTA per (tile of 32 (nu1,nu2) elements, target pair x column chunk, q).
+// Warps: 4 along rows (16 rows each) x WN along the (l1,l2) columns, TN n8
+// tiles each; BN = 8 TN WN >= Nl^2 (or a chunk of it).
+template <int TN, int WN>
+__global__ void __launch_bounds__(128 * WN) k_pae_mma(PaePtrs P, const int* __restrict__ ibz,
+                                                      const int* __restrict__ signs, int Nz, int Nf, int Nl, int NIBZ,
+                                                      int NR, int nchunks, double aux, double inv_nx) {
+  constexpr int BN = 8 * TN * WN;
+  constexpr int NT = 128 * WN;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  cplx* sA = reinterpret_cast<cplx*>(smraw);      // [2][BK][LDA]
+  cplx* sB = sA + 2 * PAE_BK * PAE_LDA;           // [2][BN][LDB]
+  __shared__ int e_w2[2][PAE_E], e_a[2][PAE_E], e_b[2][PAE_E], e_tr[2][PAE_E];
+  __shared__ double s_sg[16];
+
+  const int tile = blockIdx.x;
+  const int pair = blockIdx.y / nchunks, chunk = blockIdx.y % nchunks;
+  const int q = blockIdx.z;
   const int W = ibz[3 * q + 2];
   const int Qi = q / (Nf / 2);
   const int nh = Nf / 2;
-  const size_t n2 = (size_t)Nz * Nz;
   const int nl2 = Nl * Nl, nl4 = nl2 * nl2;
-  // targets and sources: pair 0 -> (F_d, F_m), sources (d,m) for types 0,1 and
-  // (s,t) for types 2,3; pair 1 -> (F_s, F_t), sources (d,m) for all types
-  const int ta = pair == 0 ? 0 : 2, tb = ta + 1;
-  // dispatch factors (SRC/parquet_EQOuter.f90:84-113): [type][source][target]
-  double fac[4][2][2];
-  if (pair == 0) {
-    const double f01[2][2] = {{-0.5, -0.5}, {-1.5, 0.5}};  // phbar_to_ph from d, m
-    const double f23[2][2] = {{0.5, -0.5}, {1.5, 0.5}};    // pp_to_ph from s, t
-    for (int s = 0; s < 2; s++)
-      for (int g = 0; g < 2; g++) {
-        fac[0][s][g] = fac[1][s][g] = f01[s][g];
-        fac[2][s][g] = fac[3][s][g] = f23[s][g];
-      }
-  } else {
-    const double f01[2][2] = {{0.5, 0.5}, {-1.5, 0.5}};    // ph_to_pp from d, m
-    const double f23[2][2] = {{0.5, -0.5}, {-1.5, -0.5}};  // phbar_to_pp from d, m
-    for (int s = 0; s < 2; s++)
-      for (int g = 0; g < 2; g++) {
-        fac[0][s][g] = fac[1][s][g] = f01[s][g];
-        fac[2][s][g] = fac[3][s][g] = f23[s][g];
-      }
-  }
-  // M type of each contribution
-  const int mtype[4] = {pair == 0 ? 0 : 2, pair == 0 ? 0 : 2, pair == 0 ? 1 : 3, pair == 0 ? 1 : 3};
+  const int KF = nl2 * NR;  // k per family
+  const int K = 2 * KF;
+  const size_t n2 = (size_t)Nz * Nz;
+  const int tid = threadIdx.x;
 
-  for (int e = threadIdx.x; e < Nf * Nf; e += blockDim.x) {
-    const int nu1 = e % Nf + 1, nu2 = e / Nf + 1;
-    cplx acc_a[PAE_NLMAX], acc_b[PAE_NLMAX];
-#pragma unroll
-    for (int l2 = 0; l2 < PAE_NLMAX; l2++) acc_a[l2] = acc_b[l2] = cmk(0.0, 0.0);
-    for (int t = 0; t < 4; t++) {
-      int w2, a, b;
-      if (!pae_map(pair, t, nu1, nu2, W, Nf, &w2, &a, &b)) continue;
-      const bool tr = t & 1;
-      const int s0 = (pair == 0 && t >= 2) ? 2 : 0;  // first source channel
-      const cplx* X0 = P.PhiR[s0] + n2 * (w2 - 1);
-      const cplx* X1 = P.PhiR[s0 + 1] + n2 * (w2 - 1);
-      const cplx* Mt = P.M[mtype[t]] + (size_t)nl4 * Qi;
-      const double fa0 = fac[t][0][0], fa1 = fac[t][1][0], fb0 = fac[t][0][1], fb1 = fac[t][1][1];
-      for (int R = 0; R < NR; R++) {
-        const size_t roff = n2 * nh * R;
-        const cplx* MR = Mt + (size_t)nl4 * NIBZ * R;
-        for (int l4 = 0; l4 < Nl; l4++)
-          for (int l3 = 0; l3 < Nl; l3++) {
-            const size_t xi = (size_t)(l3 * Nf + a - 1) + (size_t)Nz * (l4 * Nf + b - 1) + roff;
-            cplx x0 = X0[xi], x1 = X1[xi];
-            if (tr) {
-              const double sg = (double)(signs[l3] * signs[l4]);
-              x0 = cscale(cconj(x0), sg);
-              x1 = cscale(cconj(x1), sg);
-            }
-            const cplx xa = cmk(fa0 * x0.x + fa1 * x1.x, fa0 * x0.y + fa1 * x1.y);
-            const cplx xb = cmk(fb0 * x0.x + fb1 * x1.x, fb0 * x0.y + fb1 * x1.y);
-            const cplx* Mrow = MR + l1 + (size_t)nl2 * (l3 + Nl * l4);
-#pragma unroll
-            for (int l2 = 0; l2 < PAE_NLMAX; l2++) {
-              if (l2 < Nl) {
-                const cplx m = __ldg(Mrow + Nl * l2);
-                acc_a[l2] = cfma(m, xa, acc_a[l2]);
-                acc_b[l2] = cfma(m, xb, acc_b[l2]);
-              }
-            }
-          }
-      }
-    }
-    // F = Phi + Lambda*Nc on the l=1 block + contributions/Nx
-    const size_t i = (size_t)(l1 * Nf + nu1 - 1);
-#pragma unroll
-    for (int l2 = 0; l2 < PAE_NLMAX; l2++) {
-      if (l2 < Nl) {
-        const size_t idx = i + (size_t)Nz * (l2 * Nf + nu2 - 1) + n2 * q;
-        cplx fa = P.Phi[ta][idx], fb = P.Phi[tb][idx];
-        if (l1 == 0 && l2 == 0) {
-          const size_t li = (size_t)(nu1 - 1) + (size_t)Nf * ((nu2 - 1) + (size_t)Nf * (W - 1));
-          fa = cadd(fa, cscale(P.L[ta][li], aux));
-          fb = cadd(fb, cscale(P.L[tb][li], aux));
-        }
-        P.F[ta][idx] = cadd(fa, cscale(acc_a[l2], inv_nx));
-        P.F[tb][idx] = cadd(fb, cscale(acc_b[l2], inv_nx));
-      }
-    }
+  // per-element family maps
+  if (tid < 2 * PAE_E) {
+    const int fam = tid / PAE_E, e = tid % PAE_E;
+    const int g = tile * PAE_E + e;
+    int w2 = 0, a = 1, b = 1, tr = 0;
+    bool ok = g < Nf * Nf && pae_family(pair, fam, g % Nf + 1, g / Nf + 1, W, Nf, &w2, &a, &b, &tr);
+    e_w2[fam][e] = ok ? w2 : 0;
+    e_a[fam][e] = a;
+    e_b[fam][e] = b;
+    e_tr[fam][e] = tr;
   }
+  if (tid < Nl) s_sg[tid] = (double)signs[tid];
+  // dispatch factors fac[fam][source][target] (SRC/parquet_EQOuter.f90:84-113)
+  // and the first source channel of each family
+  __shared__ double fac[2][2][2];
+  __shared__ int src0[2];
+  if (tid == 0) {
+    // pair 0: D = phbar_to_ph from (d, m), A = pp_to_ph from (s, t)
+    // pair 1: D = phbar_to_pp from (d, m), A = ph_to_pp from (d, m)
+    const double f0[2][2][2] = {{{-0.5, -0.5}, {-1.5, 0.5}}, {{0.5, -0.5}, {1.5, 0.5}}};
+    const double f1[2][2][2] = {{{0.5, -0.5}, {-1.5, -0.5}}, {{0.5, 0.5}, {-1.5, 0.5}}};
+    for (int x = 0; x < 2; x++)
+      for (int y = 0; y < 2; y++)
+        for (int z = 0; z < 2; z++) fac[x][y][z] = pair == 0 ? f0[x][y][z] : f1[x][y][z];
+    src0[0] = 0;
+    src0[1] = pair == 0 ? 2 : 0;
+  }
+  const cplx* Mf[2] = {P.M[pair == 0 ? 0 : 3], P.M[pair == 0 ? 1 : 2]};
+  __syncthreads();
+
+  // gather of one K step into registers: thread -> (element, kk) pairs
+  constexpr int APER = PAE_E * PAE_BK / NT > 0 ? PAE_E * PAE_BK / NT : 1;
+  cplx ra[APER], rb[APER];
+  auto gather = [&](int kt) {
+#pragma unroll
+    for (int i = 0; i < APER; i++) {
+      const int p = tid + i * NT;
+      ra[i] = rb[i] = cmk(0.0, 0.0);
+      if (p >= PAE_E * PAE_BK) continue;
+      const int e = p % PAE_E, kk = p / PAE_E;
+      const int k = kt * PAE_BK + kk;
+      if (k >= K) continue;
+      const int fam = k / KF, kf = k % KF;
+      const int w2 = e_w2[fam][e];
+      if (w2 == 0) continue;
+      const int l34 = kf % nl2, R = kf / nl2;
+      const int l3 = l34 % Nl, l4 = l34 / Nl;
+      const size_t xi = (size_t)(l3 * Nf + e_a[fam][e] - 1) + (size_t)Nz * (l4 * Nf + e_b[fam][e] - 1) +
+                        n2 * ((size_t)(w2 - 1) + (size_t)nh * R);
+      const int s0 = src0[fam];
+      cplx x0 = P.PhiR[s0][xi], x1 = P.PhiR[s0 + 1][xi];
+      if (e_tr[fam][e]) {
+        const double sg = s_sg[l3] * s_sg[l4];
+        x0 = cmk(sg * x0.x, -sg * x0.y);
+        x1 = cmk(sg * x1.x, -sg * x1.y);
+      }
+      ra[i] = cmk(fac[fam][0][0] * x0.x + fac[fam][1][0] * x1.x, fac[fam][0][0] * x0.y + fac[fam][1][0] * x1.y);
+      rb[i] = cmk(fac[fam][0][1] * x0.x + fac[fam][1][1] * x1.x, fac[fam][0][1] * x0.y + fac[fam][1][1] * x1.y);
+    }
+  };
+  auto store_a = [&](int stage) {
+    cplx* dA = sA + (size_t)stage * PAE_BK * PAE_LDA;
+#pragma unroll
+    for (int i = 0; i < APER; i++) {
+      const int p = tid + i * NT;
+      if (p >= PAE_E * PAE_BK) continue;
+      const int e = p % PAE_E, kk = p / PAE_E;
+      dA[kk * PAE_LDA + e] = ra[i];
+      dA[kk * PAE_LDA + PAE_E + e] = rb[i];
+    }
+  };
+  auto load_b = [&](int stage, int kt) {
+    cplx* dB = sB + (size_t)stage * BN * PAE_LDB;
+    for (int p = tid; p < BN * PAE_BK; p += NT) {
+      const int kk = p % PAE_BK, n = p / PAE_BK;
+      const int k = kt * PAE_BK + kk;
+      const int col = chunk * BN + n;
+      const bool ok = k < K && col < nl2;
+      const cplx* src = Mf[0];
+      if (ok) {
+        const int fam = k / KF, kf = k % KF;
+        const int l34 = kf % nl2, R = kf / nl2;
+        src = Mf[fam] + col + (size_t)nl2 * l34 + (size_t)nl4 * (Qi + (size_t)NIBZ * R);
+      }
+      cp_async16p(dB + n * PAE_LDB + kk, src, ok);
+    }
+    asm volatile("cp.async.commit_group;\n" ::);
+  };
+
+  const int lane = tid & 31, warp = tid >> 5;
+  const int wr = warp % 4, wc = warp / 4;
+  const int gid = lane >> 2, tig = lane & 3;
+  double cre[TN][4], cim[TN][4];
+#pragma unroll
+  for (int j = 0; j < TN; j++)
+#pragma unroll
+    for (int x = 0; x < 4; x++) cre[j][x] = cim[j][x] = 0.0;
+
+  const int ktiles = (K + PAE_BK - 1) / PAE_BK;
+  gather(0);
+  load_b(0, 0);
+  store_a(0);
+  for (int kt = 0; kt < ktiles; kt++) {
+    const int cur = kt & 1;
+    asm volatile("cp.async.wait_group 0;\n" ::);
+    __syncthreads();
+    if (kt + 1 < ktiles) {
+      gather(kt + 1);
+      load_b(cur ^ 1, kt + 1);
+    }
+    const cplx* cA = sA + (size_t)cur * PAE_BK * PAE_LDA;
+    const cplx* cB = sB + (size_t)cur * BN * PAE_LDB;
+#pragma unroll
+    for (int k8 = 0; k8 < PAE_BK; k8 += 8) {
+      double are[4], aim[4], anim[4];
+      const int mb = wr * 16 + gid;
+      const cplx v0 = cA[(k8 + tig) * PAE_LDA + mb], v1 = cA[(k8 + tig) * PAE_LDA + mb + 8];
+      const cplx v2 = cA[(k8 + tig + 4) * PAE_LDA + mb], v3 = cA[(k8 + tig + 4) * PAE_LDA + mb + 8];
+      are[0] = v0.x; aim[0] = v0.y;
+      are[1] = v1.x; aim[1] = v1.y;
+      are[2] = v2.x; aim[2] = v2.y;
+      are[3] = v3.x; aim[3] = v3.y;
+#pragma unroll
+      for (int x = 0; x < 4; x++) anim[x] = -aim[x];
+#pragma unroll
+      for (int j = 0; j < TN; j++) {
+        const int nb = (wc * TN + j) * 8 + gid;
+        const cplx w0 = cB[nb * PAE_LDB + k8 + tig], w1 = cB[nb * PAE_LDB + k8 + tig + 4];
+        const double bre[2] = {w0.x, w1.x}, bim[2] = {w0.y, w1.y};
+        dmma_16x8x8(cre[j], are, bre);
+        dmma_16x8x8(cre[j], anim, bim);
+        dmma_16x8x8(cim[j], are, bim);
+        dmma_16x8x8(cim[j], aim, bre);
+      }
+    }
+    if (kt + 1 < ktiles) store_a(cur ^ 1);
+  }
+
+  // epilogue: F = Phi + Lambda*Nc on the (l=1, l=1) block + C/Nx
+#pragma unroll
+  for (int j = 0; j < TN; j++)
+#pragma unroll
+    for (int x = 0; x < 4; x++) {
+      const int row = wr * 16 + gid + (x >= 2 ? 8 : 0);
+      const int col = chunk * BN + (wc * TN + j) * 8 + 2 * tig + (x & 1);
+      const int tgt = row / PAE_E, e = row % PAE_E;
+      const int g = tile * PAE_E + e;
+      if (col >= nl2 || g >= Nf * Nf) continue;
+      const int nu1 = g % Nf + 1, nu2 = g / Nf + 1;
+      const int l1 = col % Nl, l2 = col / Nl;
+      const int r = (pair == 0 ? 0 : 2) + tgt;
+      const size_t idx = (size_t)(l1 * Nf + nu1 - 1) + (size_t)Nz * (l2 * Nf + nu2 - 1) + n2 * q;
+      cplx f = P.Phi[r][idx];
+      if (l1 == 0 && l2 == 0) {
+        const cplx lam = P.L[r][(size_t)(nu1 - 1) + (size_t)Nf * ((nu2 - 1) + (size_t)Nf * (W - 1))];
+        f = cadd(f, cscale(lam, aux));
+      }
+      P.F[r][idx] = cmk(f.x + inv_nx * cre[j][x], f.y + inv_nx * cim[j][x]);
+    }
+}
+
+template <int TN, int WN>
+static int run_pae(tups_ctx* ctx, const PaePtrs& P, int nchunks) {
+  const auto& d = ctx->d;
+  constexpr int BN = 8 * TN * WN;
+  const size_t sm = (size_t)(2 * PAE_BK * PAE_LDA + 2 * BN * PAE_LDB) * sizeof(cplx);
+  auto kern = k_pae_mma<TN, WN>;
+  if (sm > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return cuda_check(ctx, e, "k_pae_mma smem attribute");
+  }
+  const int tiles = (d.Nf * d.Nf + PAE_E - 1) / PAE_E;
+  dim3 grid(tiles, 2 * nchunks, d.Nb);
+  kern<<<grid, 128 * WN, sm, ctx->stream>>>(P, ctx->t.ibz, ctx->t.signs, d.Nz, d.Nf, d.Nl, d.NIBZ, d.NR, nchunks,
+                                            std::fabs(1.0 / ctx->FF[0] * 1.0 / ctx->FF[0]), 1.0 / d.Nx);
+  return after_launch(ctx, "k_pae_mma");
 }
 
 int launch_pae(tups_ctx* ctx) {
   const auto& d = ctx->d;
-  if (d.Nl > PAE_NLMAX) return set_error(ctx, TUPS_ERR_BADDIM, "Nl > 13 not supported by the crossing kernel");
+  if (d.Nl > 13) return set_error(ctx, TUPS_ERR_BADDIM, "Nl > 13 not supported by the crossing kernel");
   PaePtrs P;
   for (int r = 0; r < 4; r++) {
     P.Phi[r] = ctx->s.G[r];
@@ -206,10 +333,10 @@ int launch_pae(tups_ctx* ctx) {
     P.L[r] = ctx->t.L[r];
     P.F[r] = ctx->s.F[r];
   }
-  dim3 grid(d.Nb, 2, d.Nl);
-  k_pae<<<grid, 256, 0, ctx->stream>>>(P, ctx->t.ibz, ctx->t.signs, d.Nz, d.Nf, d.Nl, d.NIBZ, d.NR,
-                                       std::fabs(1.0 / ctx->FF[0] * 1.0 / ctx->FF[0]), 1.0 / d.Nx);
-  return after_launch(ctx, "k_pae");
+  const int nl2 = d.Nl * d.Nl;
+  if (nl2 <= 8) return run_pae<1, 1>(ctx, P, 1);
+  if (nl2 <= 32) return run_pae<4, 1>(ctx, P, 1);
+  return run_pae<6, 2>(ctx, P, (nl2 + 95) / 96);
 }
 
 }  // namespace tups

@@ -666,7 +666,12 @@ static int init_state(tups_ctx* ctx) {
   return TUPS_OK;
 }
 
+namespace tups {
+void destroy_events(tups_ctx* ctx);
+}
+
 static void free_all(tups_ctx* ctx) {
+  tups::destroy_events(ctx);
   for (void* p : ctx->allocations) cudaFree(p);
   ctx->allocations.clear();
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -703,6 +708,20 @@ extern "C" int tups_ctx_destroy(tups_ctx* ctx) {
   free_all(ctx);
   delete ctx;
   return TUPS_OK;
+}
+
+extern "C" int tups_host_tables(const tups_params* p, tups_dims* d, double* FF, double* FF_inv, int* signs,
+                                int* reps, int* lsym, double* lfac, int* ibz) {
+  if (!p) return TUPS_ERR_BADARG;
+  tups_ctx tmp;
+  tmp.p = *p;
+  int rc = build_tables(&tmp);
+  if (rc != TUPS_OK) {
+    std::fprintf(stderr, "tups_host_tables: %s\n", tmp.err.c_str());
+    return rc;
+  }
+  if (d) *d = tmp.d;
+  return tups_get_tables(&tmp, FF, FF_inv, signs, reps, lsym, lfac, ibz);
 }
 
 extern "C" int tups_get_dims(const tups_ctx* ctx, tups_dims* out) {

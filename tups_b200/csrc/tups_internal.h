@@ -96,7 +96,22 @@ struct tups_ctx {
   tups::DeviceTables t;
   tups::DeviceState s;
   std::vector<void*> allocations;
+  // instrumentation: event pairs per phase, reused across calls
+  bool timing = false;
+  std::vector<cudaEvent_t> ev_begin[TUPS_NPHASE], ev_end[TUPS_NPHASE];
+  int ev_used[TUPS_NPHASE] = {};
+  double phase_ms[TUPS_NPHASE] = {};
+  int phase_count[TUPS_NPHASE] = {};
+  cudaEvent_t marks[8] = {};
 };
+
+namespace tups {
+// bracket a phase with CUDA events on the library's stream when timing is on
+void phase_begin(tups_ctx* ctx, int phase);
+void phase_end(tups_ctx* ctx, int phase);
+// fold recorded event pairs into phase_ms (synchronizes the stream)
+void phase_collect(tups_ctx* ctx);
+}  // namespace tups
 
 namespace tups {
 

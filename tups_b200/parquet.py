@@ -109,6 +109,31 @@ def _ptr(a: np.ndarray) -> C.c_void_p:
     return C.c_void_p(a.ctypes.data)
 
 
+def host_tables(params: Params) -> dict:
+    """Sizes and form-factor/symmetry/index tables built by the native host
+    code without touching a GPU (the host part of tups_ctx_create)."""
+    lib = _lib.load()
+    cp = params.to_c()
+    d = tups_dims()
+    rc = lib.tups_host_tables(C.byref(cp), C.byref(d), *([None] * 7))
+    if rc != 0:
+        raise TupsError(rc, "tups_host_tables failed (see stderr)")
+    dims = {f[0]: getattr(d, f[0]) for f in d._fields_}
+    nl, nx = dims["Nl"], dims["Nx"]
+    FF = np.empty((nx, nx, nl), order="F")
+    FFi = np.empty((8, nx, nx, nl), order="F")
+    signs = np.empty(nl, dtype=np.int32)
+    reps = np.empty(nl, dtype=np.int32)
+    lsym = np.empty((8, nl), dtype=np.int32, order="F")
+    lfac = np.empty((8, nl), order="F")
+    ibz = np.empty((3, dims["Nred"]), dtype=np.int32, order="F")
+    rc = lib.tups_host_tables(C.byref(cp), C.byref(d), *(_ptr(x) for x in (FF, FFi, signs, reps, lsym, lfac, ibz)))
+    if rc != 0:
+        raise TupsError(rc, "tups_host_tables failed")
+    return {"dims": dims, "FF": FF, "FF_inv": FFi, "signs": signs, "reps": reps, "lsym": lsym, "lfac": lfac,
+            "ibz": ibz.T.copy()}
+
+
 class Solver:
     """One parquet solver instance with device-resident state."""
 
@@ -225,6 +250,35 @@ class Solver:
 
     def synchronize(self) -> None:
         self._call("tups_synchronize")
+
+    # -- instrumentation --
+    def set_timing(self, enable: bool) -> None:
+        self._call("tups_set_timing", int(bool(enable)))
+
+    def phase_times(self) -> dict:
+        """Accumulated device milliseconds and launch counts per phase."""
+        ms = (C.c_double * len(_lib.PHASES))()
+        cnt = (C.c_int * len(_lib.PHASES))()
+        self._call("tups_get_phase_times", C.cast(ms, C.c_void_p), C.cast(cnt, C.c_void_p))
+        return {p: (ms[i], cnt[i]) for i, p in enumerate(_lib.PHASES)}
+
+    def record_event(self, slot: int) -> None:
+        self._call("tups_record_event", int(slot))
+
+    def event_elapsed_ms(self, a: int, b: int) -> float:
+        v = C.c_double()
+        self._call("tups_event_elapsed", int(a), int(b), C.byref(v))
+        return v.value
+
+    def get_sigma_into(self, out: np.ndarray) -> None:
+        """D2H of Sigma into a caller-owned (e.g. pinned) complex128 buffer."""
+        assert out.dtype == np.complex128 and out.size == self.Nt and out.flags.c_contiguous
+        self._call("tups_get_sigma", _ptr(out))
+
+    def set_sigma_from(self, buf: np.ndarray) -> None:
+        """H2D of Sigma from a caller-owned (e.g. pinned) complex128 buffer."""
+        assert buf.dtype == np.complex128 and buf.size == self.Nt and buf.flags.c_contiguous
+        self._call("tups_set_sigma", _ptr(buf))
 
     # -- state in reference layouts --
     @property
