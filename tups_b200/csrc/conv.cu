@@ -75,6 +75,27 @@ __global__ void k_vertex_update(cplx* __restrict__ G0, cplx* __restrict__ G1, cp
     G[i] = csub(F[i], G[i]);
 }
 
+// F = G = value on the (l=1, l=1) nu-block of every slot (SRC/preprocessing.f90:102-116)
+__global__ void k_fill_lambda_block(cplx* __restrict__ F, cplx* __restrict__ G, int Nz, int Nf, int Nb,
+                                    double value) {
+  const size_t n = (size_t)Nf * Nf * Nb;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(e % Nf), j = (int)((e / Nf) % Nf);
+    const size_t q = e / ((size_t)Nf * Nf);
+    const size_t idx = i + (size_t)Nz * (j + (size_t)Nz * q);
+    F[idx] = cmk(value, 0.0);
+    G[idx] = cmk(value, 0.0);
+  }
+}
+
+int launch_fill_lambda_block(tups_ctx* ctx, cplx* F, cplx* G, double value) {
+  const auto& d = ctx->d;
+  const size_t n = (size_t)d.Nf * d.Nf * d.Nb;
+  k_fill_lambda_block<<<(unsigned)std::min<size_t>(cdiv(n, 256), 148 * 8), 256, 0, ctx->stream>>>(F, G, d.Nz, d.Nf,
+                                                                                                d.Nb, value);
+  return after_launch(ctx, "k_fill_lambda_block");
+}
+
 int launch_conv(tups_ctx* ctx) {
   const auto& d = ctx->d;
   k_conv_sigma<<<1, 1024, 0, ctx->stream>>>(ctx->s.Sigma, ctx->s.SigmaOld, ctx->s.scal, d.Nt);

@@ -622,21 +622,16 @@ static int alloc_state(tups_ctx* ctx) {
 static int init_state(tups_ctx* ctx) {
   const tups_dims& d = ctx->d;
   auto& s = ctx->s;
-  const size_t Nz = d.Nz, Nb = d.Nb, Nf = d.Nf;
+  const size_t Nz = d.Nz, Nb = d.Nb;
   const double U = ctx->p.U;
   const double lam[4] = {U, -U, 2.0 * U, 0.0};
-  std::vector<cplx> v(Nz * Nz * Nb);
   for (int r = 0; r < 4; r++) {
-    std::fill(v.begin(), v.end(), make_double2(0.0, 0.0));
-    double val = lam[r] * ctx->aux;
-    for (size_t q = 0; q < Nb; q++)
-      for (size_t j = 0; j < Nf; j++)
-        for (size_t i = 0; i < Nf; i++) v[i + Nz * (j + Nz * q)] = make_double2(val, 0.0);
-    TRY(tups::cuda_check(ctx, cudaMemcpy(s.F[r], v.data(), v.size() * sizeof(cplx), cudaMemcpyHostToDevice),
-                         "init F"));
-    TRY(tups::cuda_check(ctx, cudaMemcpy(s.G[r], v.data(), v.size() * sizeof(cplx), cudaMemcpyHostToDevice),
-                         "init G"));
+    const size_t bytes = Nz * Nz * Nb * sizeof(cplx);
+    TRY(tups::cuda_check(ctx, cudaMemsetAsync(s.F[r], 0, bytes, ctx->stream), "init F"));
+    TRY(tups::cuda_check(ctx, cudaMemsetAsync(s.G[r], 0, bytes, ctx->stream), "init G"));
+    TRY(tups::launch_fill_lambda_block(ctx, s.F[r], s.G[r], lam[r] * ctx->aux));
   }
+  TRY(tups::cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "init vertices"));
   std::vector<cplx> sig((size_t)d.Nt, make_double2(0.0, 0.0));
   if (ctx->p.use_sig_dmft) {
     // SRC/parquet_util.f90:212-230: Sigma(k, nu) = i * (third column)

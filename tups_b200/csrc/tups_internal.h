@@ -136,5 +136,6 @@ int launch_vertex_update(tups_ctx* ctx);
 int launch_output_mu(tups_ctx* ctx);
 int launch_fft2d(tups_ctx* ctx, const cplx* in, cplx* out, int forward);
 int launch_chi_aux(tups_ctx* ctx);
+int launch_fill_lambda_block(tups_ctx* ctx, cplx* F, cplx* G, double value);
 
 }  // namespace tups
