@@ -302,7 +302,7 @@ def run_tups(args, wl_name: str, wl: dict):
     ms_p, c_p = phases["pae"]
     if c_p:
         fl = 8.0 * 2 * Nl ** 4 * NR * n_valid / (c_p / K)
-        kern["k_pae"] = {"ms": ms_p, "launches": c_p, "bound": "tensor", "unit": "TFLOP/s",
+        kern["k_pae_mma"] = {"ms": ms_p, "launches": c_p, "bound": "tensor", "unit": "TFLOP/s",
                          "achieved": fl / (ms_p / c_p * 1e-3) / 1e12, "peak": peak64,
                          "peak_source": "FP64 cuBLAS ZGEMM 4096^3 measured in this run (FP64 pipe)"}
     ms_r, c_r = phases["phir"]
