@@ -194,6 +194,24 @@ int tups_synchronize(tups_ctx* ctx);
 /* number of this library's kernels launched since context creation */
 long long tups_kernel_launches(const tups_ctx* ctx);
 
+/* ---- BSE update without device allocation ----------------------------------
+ * No counterpart in the reference.  For callers that may not allocate device
+ * memory while they call this library (a host that gives all device memory
+ * to its own arena at start-up, or a loop that must not trigger the implicit
+ * synchronisation of cudaMalloc/cudaFree): the same update as BSE(ite) for
+ * n_inst (q, channel) instances that the caller owns on the device,
+ *   Phi = scale [(Gamma chi) F + F (chi Gamma)] + (1 - f_damping)(F - Gamma),
+ * written over Gamma.  gamma_phi, F: n_inst consecutive (Nz, Nz) column-major
+ * complex128 matrices; chi: n_inst consecutive (Nl, Nl, Nf) nu-diagonal blocks
+ * (chi_LL[(l1,nu),(l2,nu)] at l1 + Nl*(l2 + Nl*nu)); scale = c_r f/(beta Nx Ny)
+ * (c = 1/2, 1/2, -1/4, 1/4 for d, m, s, t); stream: a cudaStream_t or NULL.
+ * Limit: Nz <= 1024.  The scratch is a fixed 32 MiB static device array that
+ * every GPU loading the library holds until exit; the first call on a device
+ * looks up its address (make it before any stream capture); calls that
+ * overlap on the GPU race on it.  Allocates nothing; returns after queueing. */
+int tups_bse_noalloc(int n_inst, int Nz, int Nf, int Nl, double* gamma_phi, const double* F, const double* chi,
+                     double scale, double f_damping, void* stream);
+
 /* ---- instrumentation (the per-phase timings of SRC/loop.f90:64-178, taken
  * with CUDA events on the library's stream) ---------------------------------- */
 #define TUPS_PHASE_GREEN 0     /* calc_Gkw_Grt */

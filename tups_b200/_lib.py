@@ -91,6 +91,8 @@ _PROTOS = {
     "tups_get_tables": [C.c_void_p] + [C.c_void_p] * 7,
     "tups_get_sde_aux": [C.c_void_p] + [C.c_void_p] * 5,
     "tups_synchronize": [C.c_void_p],
+    "tups_bse_noalloc": [C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
+                         C.c_double, C.c_void_p],
     "tups_set_timing": [C.c_void_p, C.c_int],
     "tups_get_phase_times": [C.c_void_p, C.c_void_p, C.c_void_p],
     "tups_record_event": [C.c_void_p, C.c_int],
