@@ -111,7 +111,8 @@ __device__ __forceinline__ void dmma_16x8x8(double* c, const double* a, const do
       : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
 
-constexpr int PAE_E = 32;          // elements per CTA
+constexpr int PAE_E = 32;          // elements per CTA: an 8 (nu1) x 4 (nu2) block
+constexpr int PAE_TX = 8, PAE_TY = 4;
 constexpr int PAE_ROWS = 2 * PAE_E;  // (target, element) rows
 constexpr int PAE_BK = 16;
 constexpr int PAE_LDA = PAE_ROWS + 2;
@@ -121,7 +122,14 @@ constexpr int PAE_LDB = PAE_BK + 4;
 // Warps: 4 along rows (16 rows each) x WN along the (l1,l2) columns, TN n8
 // tiles each; BN = 8 TN WN >= Nl^2 (or a chunk of it).
 template <int TN, int WN>
-__global__ void __launch_bounds__(128 * WN) k_pae_mma(PaePtrs P, const int* __restrict__ ibz,
+#ifndef PAE_MIN_BLOCKS
+// CTAs per SM requested from ptxas for the 8-warp, 2-tile config: 3 (80
+// registers, a few spilled) runs the 8x8 / Nl=5 loop's crossing step in
+// 2.35 ms against 3.95 ms at 1 (126 registers, 2 CTAs/SM) on a B200
+#define PAE_MIN_BLOCKS 3
+#endif
+__global__ void __launch_bounds__(128 * WN, WN == 2 && TN <= 2 ? PAE_MIN_BLOCKS : 1)
+    k_pae_mma(PaePtrs P, const int* __restrict__ ibz,
                                                       const int* __restrict__ signs, int Nz, int Nf, int Nl, int NIBZ,
                                                       int NR, int nchunks, double aux, double inv_nx) {
   constexpr int BN = 8 * TN * WN;
@@ -132,9 +140,12 @@ __global__ void __launch_bounds__(128 * WN) k_pae_mma(PaePtrs P, const int* __re
   __shared__ int e_w2[2][PAE_E], e_a[2][PAE_E], e_b[2][PAE_E], e_tr[2][PAE_E];
   __shared__ double s_sg[16];
 
-  const int tile = blockIdx.x;
+  const int tiles_x = (Nf + PAE_TX - 1) / PAE_TX;
+  const int nu1_0 = (blockIdx.x % tiles_x) * PAE_TX, nu2_0 = (blockIdx.x / tiles_x) * PAE_TY;
   const int pair = blockIdx.y / nchunks, chunk = blockIdx.y % nchunks;
-  const int q = blockIdx.z;
+  // slots ordered with the bosonic frequency outermost, so that the CTAs in
+  // flight share the same band of Phi(R) in L2
+  const int q = (blockIdx.z % NIBZ) * (Nf / 2) + blockIdx.z / NIBZ;
   const int W = ibz[3 * q + 2];
   const int Qi = q / (Nf / 2);
   const int nh = Nf / 2;
@@ -144,17 +155,24 @@ __global__ void __launch_bounds__(128 * WN) k_pae_mma(PaePtrs P, const int* __re
   const size_t n2 = (size_t)Nz * Nz;
   const int tid = threadIdx.x;
 
-  // per-element family maps
+  // per-element family maps, and whether the tile is reached by each family
+  int reach0 = 0, reach1 = 0;
   if (tid < 2 * PAE_E) {
     const int fam = tid / PAE_E, e = tid % PAE_E;
-    const int g = tile * PAE_E + e;
+    const int nu1 = nu1_0 + e % PAE_TX + 1, nu2 = nu2_0 + e / PAE_TX + 1;
     int w2 = 0, a = 1, b = 1, tr = 0;
-    bool ok = g < Nf * Nf && pae_family(pair, fam, g % Nf + 1, g / Nf + 1, W, Nf, &w2, &a, &b, &tr);
+    bool ok = nu1 <= Nf && nu2 <= Nf && pae_family(pair, fam, nu1, nu2, W, Nf, &w2, &a, &b, &tr);
     e_w2[fam][e] = ok ? w2 : 0;
     e_a[fam][e] = a;
     e_b[fam][e] = b;
     e_tr[fam][e] = tr;
+    if (ok) {
+      if (fam == 0) reach0 = 1;
+      else reach1 = 1;
+    }
   }
+  const int anyD = __syncthreads_or(reach0);
+  const int anyA = __syncthreads_or(reach1);
   if (tid < Nl) s_sg[tid] = (double)signs[tid];
   // dispatch factors fac[fam][source][target] (SRC/parquet_EQOuter.f90:84-113)
   // and the first source channel of each family
@@ -194,7 +212,7 @@ __global__ void __launch_bounds__(128 * WN) k_pae_mma(PaePtrs P, const int* __re
       const size_t xi = (size_t)(l3 * Nf + e_a[fam][e] - 1) + (size_t)Nz * (l4 * Nf + e_b[fam][e] - 1) +
                         n2 * ((size_t)(w2 - 1) + (size_t)nh * R);
       const int s0 = src0[fam];
-      cplx x0 = P.PhiR[s0][xi], x1 = P.PhiR[s0 + 1][xi];
+      cplx x0 = __ldg(P.PhiR[s0] + xi), x1 = __ldg(P.PhiR[s0 + 1] + xi);
       if (e_tr[fam][e]) {
         const double sg = s_sg[l3] * s_sg[l4];
         x0 = cmk(sg * x0.x, -sg * x0.y);
@@ -242,15 +260,20 @@ __global__ void __launch_bounds__(128 * WN) k_pae_mma(PaePtrs P, const int* __re
 #pragma unroll
     for (int x = 0; x < 4; x++) cre[j][x] = cim[j][x] = 0.0;
 
-  const int ktiles = (K + PAE_BK - 1) / PAE_BK;
-  gather(0);
-  load_b(0, 0);
-  store_a(0);
-  for (int kt = 0; kt < ktiles; kt++) {
-    const int cur = kt & 1;
+  // K steps: skip the half of K that belongs to a family reaching no element
+  // of this tile (its X block is zero)
+  const int kt_lo = anyD ? 0 : KF / PAE_BK;
+  const int kt_hi = anyA ? (K + PAE_BK - 1) / PAE_BK : (KF + PAE_BK - 1) / PAE_BK;
+  if (kt_lo < kt_hi) {
+    gather(kt_lo);
+    load_b(0, kt_lo);
+    store_a(0);
+  }
+  for (int kt = kt_lo; kt < kt_hi; kt++) {
+    const int cur = (kt - kt_lo) & 1;
     asm volatile("cp.async.wait_group 0;\n" ::);
     __syncthreads();
-    if (kt + 1 < ktiles) {
+    if (kt + 1 < kt_hi) {
       gather(kt + 1);
       load_b(cur ^ 1, kt + 1);
     }
@@ -279,10 +302,12 @@ __global__ void __launch_bounds__(128 * WN) k_pae_mma(PaePtrs P, const int* __re
         dmma_16x8x8(cim[j], aim, bre);
       }
     }
-    if (kt + 1 < ktiles) store_a(cur ^ 1);
+    if (kt + 1 < kt_hi) store_a(cur ^ 1);
   }
 
-  // epilogue: F = Phi + Lambda*Nc on the (l=1, l=1) block + C/Nx
+  // epilogue: F = Phi + Lambda*Nc on the (l=1, l=1) block + C/Nx.  Phi and F
+  // are touched once: streaming loads/stores keep them from evicting Phi(R)
+  // and M from L2.
 #pragma unroll
   for (int j = 0; j < TN; j++)
 #pragma unroll
@@ -290,18 +315,17 @@ __global__ void __launch_bounds__(128 * WN) k_pae_mma(PaePtrs P, const int* __re
       const int row = wr * 16 + gid + (x >= 2 ? 8 : 0);
       const int col = chunk * BN + (wc * TN + j) * 8 + 2 * tig + (x & 1);
       const int tgt = row / PAE_E, e = row % PAE_E;
-      const int g = tile * PAE_E + e;
-      if (col >= nl2 || g >= Nf * Nf) continue;
-      const int nu1 = g % Nf + 1, nu2 = g / Nf + 1;
+      const int nu1 = nu1_0 + e % PAE_TX + 1, nu2 = nu2_0 + e / PAE_TX + 1;
+      if (col >= nl2 || nu1 > Nf || nu2 > Nf) continue;
       const int l1 = col % Nl, l2 = col / Nl;
       const int r = (pair == 0 ? 0 : 2) + tgt;
       const size_t idx = (size_t)(l1 * Nf + nu1 - 1) + (size_t)Nz * (l2 * Nf + nu2 - 1) + n2 * q;
-      cplx f = P.Phi[r][idx];
+      cplx f = __ldcs(P.Phi[r] + idx);
       if (l1 == 0 && l2 == 0) {
         const cplx lam = P.L[r][(size_t)(nu1 - 1) + (size_t)Nf * ((nu2 - 1) + (size_t)Nf * (W - 1))];
         f = cadd(f, cscale(lam, aux));
       }
-      P.F[r][idx] = cmk(f.x + inv_nx * cre[j][x], f.y + inv_nx * cim[j][x]);
+      __stcs(P.F[r] + idx, cmk(f.x + inv_nx * cre[j][x], f.y + inv_nx * cim[j][x]));
     }
 }
 
@@ -315,7 +339,7 @@ static int run_pae(tups_ctx* ctx, const PaePtrs& P, int nchunks) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return cuda_check(ctx, e, "k_pae_mma smem attribute");
   }
-  const int tiles = (d.Nf * d.Nf + PAE_E - 1) / PAE_E;
+  const int tiles = ((d.Nf + PAE_TX - 1) / PAE_TX) * ((d.Nf + PAE_TY - 1) / PAE_TY);
   dim3 grid(tiles, 2 * nchunks, d.Nb);
   kern<<<grid, 128 * WN, sm, ctx->stream>>>(P, ctx->t.ibz, ctx->t.signs, d.Nz, d.Nf, d.Nl, d.NIBZ, d.NR, nchunks,
                                             std::fabs(1.0 / ctx->FF[0] * 1.0 / ctx->FF[0]), 1.0 / d.Nx);
@@ -335,7 +359,7 @@ int launch_pae(tups_ctx* ctx) {
   }
   const int nl2 = d.Nl * d.Nl;
   if (nl2 <= 8) return run_pae<1, 1>(ctx, P, 1);
-  if (nl2 <= 32) return run_pae<4, 1>(ctx, P, 1);
+  if (nl2 <= 32) return run_pae<2, 2>(ctx, P, 1);
   return run_pae<6, 2>(ctx, P, (nl2 + 95) / 96);
 }
 
