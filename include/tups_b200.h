@@ -158,10 +158,26 @@ int tups_vertex_update(tups_ctx* ctx);
 /* the every-5-iterations readout's effect on the trajectory (SRC/loop.f90:195,
  * SRC/parquet_chi.f90:114-122): mu <- midpoint of [mu-U, mu+U] */
 int tups_output_block(tups_ctx* ctx);
-/* one pass of execute_loop (SRC/loop.f90:51-244) without HDF5 output */
+/* one pass of execute_loop (SRC/loop.f90:51-244) without the readout: on
+ * output iterations only the readout's effect on mu is applied */
 int tups_iteration(tups_ctx* ctx, int ite, tups_conv_info* info);
-/* execute_loop (SRC/loop.f90:29-249); *ite_out = iterations done */
+/* execute_loop (SRC/loop.f90:29-249) including the readout of every output
+ * iteration (SRC/loop.f90:181-213; results via tups_get_chi0/tups_get_sus);
+ * *ite_out = iterations done */
 int tups_execute_loop(tups_ctx* ctx, int* ite_out, int* converged);
+
+/* ---- readout (SRC/loop.f90:181-213 without HDF5) -------------------------- */
+/* calc_Gkw_Grt(ite, Grt, .true.) with the exact chi0 bubble
+ * (SRC/parquet_chi.f90:216-430), calc_sus (SRC/parquet_sus.f90:18-643) and
+ * symmetrize_sus (SRC/parquet_plot.f90:14-58).  Call between tups_conv and
+ * tups_vertex_update, as the reference does. */
+int tups_readout(tups_ctx* ctx, int ite);
+/* chi0 of the last readout. bz = 0: IBZ arrays chi0_ph, chi0_pp (Nred) and
+ * chi0_ph_FF, chi0_pp_FF (Nred, 4); bz = 1: the whole-BZ versions
+ * (Nx*Ny*Nf/2) and (Nx*Ny*Nf/2, 4).  Any pointer may be NULL. */
+int tups_get_chi0(tups_ctx* ctx, int bz, double* ph, double* pp, double* ph_FF, double* pp_FF);
+/* sus_r of the last readout: bz = 0 sus_r_IBZ (Nred, 4), bz = 1 sus_r (Nx*Ny*Nf/2, 4) */
+int tups_get_sus(tups_ctx* ctx, int channel, int bz, double* host);
 
 /* ---- state in/out (host buffers, reference layouts) ------------------ */
 int tups_get_sigma(tups_ctx* ctx, double* sigma);         /* (Nt) */

@@ -1381,6 +1381,171 @@ def conv(st: State) -> tuple[bool, dict]:
     return conv_ok, out
 
 
+# --------------------------------------------------------------------------
+# readout every 5 iterations: exact chi0 bubble and susceptibilities
+# (parquet_chi.f90:216-430, parquet_sus.f90:18-643, parquet_plot.f90:14-58)
+# --------------------------------------------------------------------------
+def grt_pre_fft(st: State) -> np.ndarray:
+    """G(k, tau) on the fine grid before the spatial FFT, for the current mu
+    and Sigma (parquet_chi.f90:124-174 / :355-390)."""
+    Nx, Ny, Nf, Ng, beta, mu = st.Nx, st.Ny, st.Nf, st.Ng, st.p.beta, st.mu
+    Sig = st.Sigma.reshape(Nx, Ny, Nf)
+    nu = np.arange(1, Nf + 1)
+    fr = freq(st, nu)
+    tau = beta / (Nf - 1) * (np.arange(1, Nf + 1) - 1)
+    ph = -math.pi / beta * (2.0 * (nu - Nf // 2) - 1.0)
+    tw = np.exp(1j * (ph[None, :] * tau[:, None]))
+    out = np.zeros((Nx * Ng, Ny * Ng, Nf), dtype=np.complex128)
+    src = np.zeros((Nx * Ng, Ny * Ng), dtype=np.int64)  # coarse k of each fine point
+    for ky in range(1, Ny + 1):
+        for kx in range(1, Nx + 1):
+            for kyc in range(1, Ng + 1):
+                for kxc in range(1, Ng + 1):
+                    i1 = _grain_index(kx, kxc, Nx, Ng)
+                    i2 = _grain_index(ky, kyc, Ny, Ng)
+                    e = st.Ek_grain[kxc - 1, kyc - 1, kx - 1, ky - 1]
+                    gc = 1.0 / (fr + mu - e - Sig[kx - 1, ky - 1, :])
+                    d1 = gc - 1.0 / (fr + mu - e)
+                    dummy = np.sum((tw * d1[None, :]).real / beta, axis=1)
+                    out[i1 - 1, i2 - 1, :] = dummy - np.exp((beta - tau) * (e - mu)) / (1.0 + np.exp(beta * (e - mu)))
+                    src[i1 - 1, i2 - 1] = (kx - 1) * Ny + (ky - 1)
+    return out, src
+
+
+def _bosonic_ibz(st: State, data: np.ndarray) -> np.ndarray:
+    """Spline transform tau -> bosonic frequencies at the IBZ points of a
+    fine-grid (n1, n2, Nf) array (parquet_chi.f90:242-257)."""
+    Nf, Ng = st.Nf, st.Ng
+    out = np.zeros(st.Nred, dtype=np.complex128)
+    for i in range(1, st.Nx_IBZ + 1):
+        for j in range(1, i + 1):
+            g = data[(i - 1) * Ng, (j - 1) * Ng, :].real
+            fd1, fd2 = fdfit(g, st.p.beta / float(Nf - 1))
+            c = nfourier(False, Nf - 1, Nf // 2, fd1, fd2, g, st.p.beta)
+            base = ((i * (i - 1)) // 2 + j - 1) * (Nf // 2)
+            out[base:base + Nf // 2] = c
+    return out
+
+
+def _mirror(a: np.ndarray) -> np.ndarray:
+    """a(-r, beta - tau): index 1 stays, idx -> n - idx + 2 (1-based), tau reversed."""
+    n1, n2 = a.shape[0], a.shape[1]
+    m1 = np.array([0] + [n1 - k for k in range(1, n1)])
+    m2 = np.array([0] + [n2 - k for k in range(1, n2)])
+    return a[m1[:, None], m2[None, :], :][:, :, ::-1]
+
+
+def calc_chi0_exact(st: State) -> dict:
+    """The cal_chi branch of calc_Gkw_Grt (parquet_chi.f90:216-430): Chi0_ph,
+    Chi0_pp (Nred) and the s/d-wave projected Chi0_ph_FF, Chi0_pp_FF (Nred, 4).
+    Uses the Grt of the preceding calc_Gkw_Grt(.true.) call."""
+    Grt = st.Grt
+    sd = fill_ff_sdwave(st.Nx)
+    out = {"chi0_ph": _bosonic_ibz(st, fftb2d(-Grt * _mirror(Grt))),
+           "chi0_pp": _bosonic_ibz(st, fftb2d(-0.5 * Grt ** 2))}
+    pre, src = grt_pre_fft(st)
+    ph_ff = np.zeros((st.Nred, 4), dtype=np.complex128)
+    pp_ff = np.zeros((st.Nred, 4), dtype=np.complex128)
+    sdk = sd.reshape(st.Nx * st.Ny, 4)  # k = (kx-1)*Ny + ky-1
+    for ff in range(4):
+        w = (sdk[src, ff] * sdk[src, ff])[:, :, None]
+        FFG = fftf2d(pre * w)
+        ph_ff[:, ff] = _bosonic_ibz(st, fftb2d(-Grt * _mirror(FFG)))
+        pp_ff[:, ff] = _bosonic_ibz(st, fftb2d(-0.5 * Grt * FFG))
+    out["chi0_ph_FF"] = ph_ff
+    out["chi0_pp_FF"] = pp_ff
+    return out
+
+
+def calc_GG(st: State, pp: bool) -> np.ndarray:
+    """calc_GG_ph / calc_GG_pp (parquet_sus.f90:528-643): (Nl*nbox, Nb, 4)."""
+    Nx, Ny, Nf, Ng, Nl = st.Nx, st.Ny, st.Nf, st.Ng, st.Nl
+    fr = st.p.f_range
+    nbox = (2 * fr + 1) * Nf
+    l0 = np.arange(-fr * Nf + 1, (fr + 1) * Nf + 1)
+    sd = fill_ff_sdwave(Nx)
+    kx = np.arange(Nx)[:, None, None]
+    ky = np.arange(Ny)[None, :, None]
+    nu = l0[None, None, :]
+    out = np.zeros((Nl * nbox, st.Nb, 4), dtype=np.complex128)
+    for iq in range(st.Nb):
+        qx, qy, w = (int(v) for v in st.ibz[iq])
+        g2 = np.zeros((Nx, Ny, nbox), dtype=np.complex128)
+        for gx in range(Ng):
+            for gy in range(Ng):
+                gk = green_coarse(st, gx, gy, kx, ky, nu)
+                if not pp:
+                    g2 = g2 + gk * green_coarse(st, gx, gy, (kx + qx - 1) % Nx, (ky + qy - 1) % Ny, nu + w - 1) \
+                        / Ng / Ng
+                else:
+                    mkx, mky = (-kx + Nx) % Nx, (-ky + Ny) % Ny
+                    g2 = g2 + gk * green_coarse(st, Ng - gx - 1, Ng - gy - 1, (mkx + qx - 1) % Nx,
+                                                (mky + qy - 1) % Ny, (-nu + Nf + 1) + w - 1) / Ng / Ng
+        for ff in range(4):
+            out[:, iq, ff] = np.einsum("xy,xyn,xyl->ln", sd[:, :, ff], g2, st.FF).reshape(-1)
+    return out
+
+
+def calc_sus(st: State) -> dict:
+    """calc_sus (parquet_sus.f90:18-522) at one task: sus_r_IBZ (Nred, 4).
+    Uses F_r of this iteration and Phi_r (the G arrays before the update)."""
+    Nf, Nl, Nx, Ny, beta = st.Nf, st.Nl, st.Nx, st.Ny, st.p.beta
+    fr = st.p.f_range
+    nbox = (2 * fr + 1) * Nf
+    norm = 1.0 / (Nx * Nx * Ny * Ny * beta * beta)
+    l0 = np.arange(-fr * Nf + 1, (fr + 1) * Nf + 1)
+    inb = (l0 > 0) & (l0 < Nf + 1)
+    pk = pick_range(st)
+    ff2 = 1.0 / (st.FF[0, 0, 0] * st.FF[0, 0, 0])
+    lam = {"d": st.p.U, "m": -st.p.U, "s": 2.0 * st.p.U, "t": 0.0}
+    out = {}
+    for pp, chans in ((False, "dm"), (True, "st")):
+        GG = calc_GG(st, pp)  # (Nl*nbox, Nb, 4)
+        Gb = GG.reshape(Nl, nbox, st.Nb, 4)
+        vin = Gb[:, inb, :, :].reshape(Nl * Nf, st.Nb, 4)  # in-box, index (l-1)*Nf + l0
+        for r in chans:
+            s = np.einsum("ijq,iqf,jqf->qf", st.F[r], vin, vin) * norm
+            if fr > 0:
+                # terms with at least one frequency outside the box
+                cols = (np.arange(Nl)[:, None] * Nf + (pk - 1)[None, :]).reshape(-1)
+                Phx = st.G[r][cols[:, None], cols[None, :], :]  # (Nl*nbox, Nl*nbox, Nb)
+                outside = ~(inb[:, None] & inb[None, :])
+                mask = np.tile(outside, (Nl, Nl))
+                Gv = GG  # (Nl*nbox, Nb, 4)
+                s = s + np.einsum("ijq,iqf,jqf->qf", np.where(mask[:, :, None], Phx, 0.0), Gv, Gv) * norm
+                # Lambda term on l1 = l2 = 1
+                g1 = Gb[0]  # (nbox, Nb, 4)
+                m11 = outside
+                s = s + lam[r] * ff2 * np.einsum("ij,iqf,jqf->qf", m11.astype(float), g1, g1) * norm
+            out[f"sus_{r}_IBZ"] = s
+    return out
+
+
+def symmetrize_sus(st: State, sus: dict, chi0: dict) -> dict:
+    """symmetrize_sus (parquet_plot.f90:14-58): whole-BZ arrays (Nx*Ny*Nf/2[, 4])."""
+    nh = st.Nf // 2
+    out = {}
+    for r in "dmst":
+        out[f"sus_{r}"] = np.stack([symmetrize_array(st, nh, sus[f"sus_{r}_IBZ"][:, f]) for f in range(4)], axis=1)
+    out["chi0_ph_BZ"] = symmetrize_array(st, nh, chi0["chi0_ph"])
+    out["chi0_pp_BZ"] = symmetrize_array(st, nh, chi0["chi0_pp"])
+    out["chi0_ph_BZ_FF"] = np.stack([symmetrize_array(st, nh, chi0["chi0_ph_FF"][:, f]) for f in range(4)], axis=1)
+    out["chi0_pp_BZ_FF"] = np.stack([symmetrize_array(st, nh, chi0["chi0_pp_FF"][:, f]) for f in range(4)], axis=1)
+    return out
+
+
+def readout(st: State, ite: int) -> dict:
+    """The output block of loop.f90:181-213 without HDF5: calc_Gkw_Grt(.true.),
+    calc_sus, symmetrize_sus."""
+    calc_Gkw_Grt(st, ite, True)
+    chi0 = calc_chi0_exact(st)
+    sus = calc_sus(st)
+    out = dict(chi0)
+    out.update(sus)
+    out.update(symmetrize_sus(st, sus, chi0))
+    return out
+
+
 def output_block_mu(st: State) -> None:
     """Side effect of the every-5-iterations readout on the trajectory:
     ``calc_Gkw_Grt(.true.)`` (loop.f90:195) resets mu to the midpoint of

@@ -99,6 +99,45 @@ def iteration_phases(sol, st: O.State, ite: int, errs: dict) -> dict:
     return info_o
 
 
+def readout_side_by_side(p: O.Params, full_iterations: int = 2, device: int = 0) -> dict:
+    """Run `full_iterations` iterations on both sides, then the next one up
+    to the convergence check, then the readout; returns the readout errors."""
+    from tups_b200 import Solver
+    st = O.initialize(p)
+    sol = Solver(to_solver_params(p), device=device)
+    for ite in range(full_iterations):
+        O.iteration(st, ite)
+        sol.iteration(ite)
+    ite = full_iterations
+    O.calc_Gkw_Grt(st, ite, False)
+    sol.calc_Gkw_Grt(ite, False)
+    O.bse(st, ite)
+    sol.BSE(ite)
+    O.calc_PhiR(st)
+    sol.calc_PhiR(ite)
+    O.calculate_PAE(st)
+    sol.calculate_PAE()
+    st.arrays["SigmaOld"] = st.Sigma.copy()
+    O.calc_SDE(st)
+    sol.calc_SDE(ite)
+    O.conv(st)
+    sol.conv()
+    ro = O.readout(st, ite)
+    sol.readout(ite)
+    errs = {"mu": abs(sol.mu - st.mu)}
+    for bz in (False, True):
+        c = sol.chi0(bz)
+        sfx = "_BZ" if bz else ""
+        errs["chi0_ph" + sfx] = rel(c["chi0_ph"], ro["chi0_ph_BZ" if bz else "chi0_ph"])
+        errs["chi0_pp" + sfx] = rel(c["chi0_pp"], ro["chi0_pp_BZ" if bz else "chi0_pp"])
+        errs["chi0_ph_FF" + sfx] = rel(c["chi0_ph_FF"], ro["chi0_ph_BZ_FF" if bz else "chi0_ph_FF"])
+        errs["chi0_pp_FF" + sfx] = rel(c["chi0_pp_FF"], ro["chi0_pp_BZ_FF" if bz else "chi0_pp_FF"])
+        for r in CH:
+            errs[f"sus_{r}" + sfx] = rel(sol.sus(r, bz), ro[f"sus_{r}" if bz else f"sus_{r}_IBZ"])
+    sol.close()
+    return errs
+
+
 def run_side_by_side(p: O.Params, iterations: int, device: int = 0):
     """Returns (errors per phase, oracle state, solver)."""
     from tups_b200 import Solver

@@ -140,3 +140,21 @@ def test_execute_loop_converges_like_oracle(gpu_lib):
     assert (n_g, conv_g) == (n_o, conv_o)
     assert parity.rel(sol.Sigma, st.Sigma) < E2E_TOL
     sol.close()
+
+
+@pytest.mark.parametrize("case", [
+    dict(beta=2.0, U=2.0, nParticle=1.0, Nx=4, Nf=16, neighbours=1),
+    dict(beta=2.0, U=2.0, nParticle=0.9, Nx=4, Nf=8, neighbours=2),
+    dict(beta=3.0, U=1.5, nParticle=0.95, Nx=8, Nf=8, neighbours=3, tprime=-0.2),
+    dict(beta=2.0, U=2.0, nParticle=1.0, Nx=4, Nf=10, neighbours=2, f_range=1),
+    dict(beta=2.0, U=2.0, nParticle=0.9, Nx=4, Nf=8, neighbours=2, Ngrain=3),
+], ids=["nl1", "nl5_n09", "nl9_tprime", "frange1", "ngrain3"])
+def test_readout_side_by_side(gpu_lib, case):
+    """Exact chi0 bubble (4 projections), susceptibilities of all channels,
+    IBZ and whole BZ (SRC/parquet_chi.f90:216-430, parquet_sus.f90,
+    parquet_plot.f90:14-58)."""
+    p = O.Params(f_damping=0.5, ite_max=10, **case)
+    errs = parity.readout_side_by_side(p, 2)
+    assert errs.pop("mu") == 0.0
+    bad = {k: v for k, v in errs.items() if v > PHASE_TOL}
+    assert not bad, bad

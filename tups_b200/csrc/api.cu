@@ -236,7 +236,95 @@ extern "C" int tups_output_block(tups_ctx* ctx) {
   return tups::launch_output_mu(ctx);
 }
 
+// buffers of the readout, on first use
+static int ensure_readout(tups_ctx* ctx) {
+  auto& rd = ctx->rd;
+  if (rd.ready) return TUPS_OK;
+  const auto& d = ctx->d;
+  const size_t ng = (size_t)d.Nx * d.Ngrain * d.Ny * d.Ngrain * d.Nf;
+  const size_t nh = d.Nf / 2, nbz = (size_t)d.Nc * nh;
+  auto alloc = [&](void** p, size_t bytes) {
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return tups::set_error(ctx, TUPS_ERR_OOM, "readout buffers");
+    }
+    ctx->allocations.push_back(*p);
+    return TUPS_OK;
+  };
+  TRY(alloc((void**)&rd.sd, 4 * (size_t)d.Nc * sizeof(double)));
+  TRY(alloc((void**)&rd.sd2, 4 * (size_t)d.Nc * sizeof(double)));
+  TRY(alloc((void**)&rd.pre, ng * sizeof(cplx)));
+  TRY(alloc((void**)&rd.ffg_in, 4 * ng * sizeof(cplx)));
+  TRY(alloc((void**)&rd.ffg, 4 * ng * sizeof(cplx)));
+  TRY(alloc((void**)&rd.prod, 10 * ng * sizeof(cplx)));
+  TRY(alloc((void**)&rd.prod_ft, 10 * ng * sizeof(cplx)));
+  TRY(alloc((void**)&rd.chi0, 10 * (size_t)d.Nred * sizeof(cplx)));
+  TRY(alloc((void**)&rd.chi0_bz, 10 * nbz * sizeof(cplx)));
+  TRY(alloc((void**)&rd.gph, 4 * (size_t)d.Nl * d.nbox * d.Nb * sizeof(cplx)));
+  TRY(alloc((void**)&rd.gpp, 4 * (size_t)d.Nl * d.nbox * d.Nb * sizeof(cplx)));
+  TRY(alloc((void**)&rd.sus, 16 * (size_t)d.Nb * sizeof(cplx)));
+  TRY(alloc((void**)&rd.sus_bz, 16 * nbz * sizeof(cplx)));
+  // fill_FF_sdwave (SRC/parquet_formfactors.f90:792-816), k = (kx-1)*Ny + ky-1
+  std::vector<double> sd(4 * (size_t)d.Nc), sd2(4 * (size_t)d.Nc);
+  for (int kx = 1; kx <= d.Nx; kx++)
+    for (int ky = 1; ky <= d.Ny; ky++) {
+      const double px = 2.0 / d.Nx * M_PI * (kx - 1), py = 2.0 / d.Ny * M_PI * (ky - 1);
+      const double v[4] = {1.0, std::cos(px) - std::cos(py), std::sin(px), std::sin(px) * std::sin(py)};
+      const size_t k = (size_t)(kx - 1) * d.Ny + (ky - 1);
+      for (int f = 0; f < 4; f++) {
+        sd[k + (size_t)d.Nc * f] = v[f];
+        sd2[k + (size_t)d.Nc * f] = v[f] * v[f];
+      }
+    }
+  TRY(copy_h2d(ctx, rd.sd, sd.data(), sd.size() * sizeof(double)));
+  TRY(copy_h2d(ctx, rd.sd2, sd2.data(), sd2.size() * sizeof(double)));
+  rd.ready = true;
+  return TUPS_OK;
+}
+
+static int readout_async(tups_ctx* ctx) {
+  TRY(ensure_readout(ctx));
+  TRY(green_async(ctx, 1));
+  return tups::launch_readout(ctx);
+}
+
+extern "C" int tups_readout(tups_ctx* ctx, int ite) {
+  (void)ite;
+  if (!ctx) return TUPS_ERR_BADARG;
+  TRY(set_dev(ctx));
+  TRY(readout_async(ctx));
+  TRY(device_status(ctx));
+  return TUPS_OK;
+}
+
+extern "C" int tups_get_chi0(tups_ctx* ctx, int bz, double* ph, double* pp, double* ph_FF, double* pp_FF) {
+  if (!ctx) return TUPS_ERR_BADARG;
+  if (!ctx->rd.ready) return tups::set_error(ctx, TUPS_ERR_STATE, "no readout yet");
+  const size_t n = bz ? (size_t)ctx->d.Nc * (ctx->d.Nf / 2) : (size_t)ctx->d.Nred;
+  const cplx* base = bz ? ctx->rd.chi0_bz : ctx->rd.chi0;
+  if (ph) TRY(copy_d2h(ctx, ph, base, n * sizeof(cplx)));
+  if (pp) TRY(copy_d2h(ctx, pp, base + n, n * sizeof(cplx)));
+  if (ph_FF) TRY(copy_d2h(ctx, ph_FF, base + 2 * n, 4 * n * sizeof(cplx)));
+  if (pp_FF) TRY(copy_d2h(ctx, pp_FF, base + 6 * n, 4 * n * sizeof(cplx)));
+  return TUPS_OK;
+}
+
+extern "C" int tups_get_sus(tups_ctx* ctx, int channel, int bz, double* host) {
+  if (!ctx || channel < 0 || channel > 3) return TUPS_ERR_BADARG;
+  if (!ctx->rd.ready) return tups::set_error(ctx, TUPS_ERR_STATE, "no readout yet");
+  const size_t n = bz ? (size_t)ctx->d.Nc * (ctx->d.Nf / 2) : (size_t)ctx->d.Nb;
+  const cplx* base = bz ? ctx->rd.sus_bz : ctx->rd.sus;
+  return copy_d2h(ctx, host, base + 4 * n * channel, 4 * n * sizeof(cplx));
+}
+
+static int iteration_impl(tups_ctx* ctx, int ite, tups_conv_info* info, bool with_readout);
+
 extern "C" int tups_iteration(tups_ctx* ctx, int ite, tups_conv_info* info) {
+  return iteration_impl(ctx, ite, info, false);
+}
+
+static int iteration_impl(tups_ctx* ctx, int ite, tups_conv_info* info, bool with_readout) {
   if (!ctx) return TUPS_ERR_BADARG;
   TRY(set_dev(ctx));
   // SRC/loop.f90:67 .. 222, without the HDF5 output
@@ -261,7 +349,10 @@ extern "C" int tups_iteration(tups_ctx* ctx, int ite, tups_conv_info* info) {
   int rc = tups_conv(ctx, &ci);
   if (info) *info = ci;
   if (rc) return rc;
-  if (ite % 5 == 0 || ite == ctx->p.ite_max - 1 || ci.converged) TRY(tups::launch_output_mu(ctx));
+  if (ite % 5 == 0 || ite == ctx->p.ite_max - 1 || ci.converged) {
+    if (with_readout) TRY(readout_async(ctx));
+    else TRY(tups::launch_output_mu(ctx));
+  }
   tups::phase_begin(ctx, TUPS_PHASE_UPDATE);
   TRY(tups::launch_vertex_update(ctx));
   tups::phase_end(ctx, TUPS_PHASE_UPDATE);
@@ -273,7 +364,7 @@ extern "C" int tups_execute_loop(tups_ctx* ctx, int* ite_out, int* converged) {
   int ite = 0, conv = 0;
   while (!conv && ite < ctx->p.ite_max) {
     tups_conv_info ci;
-    int rc = tups_iteration(ctx, ite, &ci);
+    int rc = iteration_impl(ctx, ite, &ci, true);
     if (rc) {
       if (ite_out) *ite_out = ite;
       return rc;

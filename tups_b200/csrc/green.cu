@@ -192,25 +192,32 @@ int launch_bisection(tups_ctx* ctx, int cal_chi, int max_steps) {
   return after_launch(ctx, "k_bisection");
 }
 
-int launch_grt(tups_ctx* ctx) {
+int launch_grt_pre(tups_ctx* ctx, cplx* out) {
   const auto& d = ctx->d;
   const int npts = d.Nc * d.Ngrain * d.Ngrain;
   k_grt_points<<<npts, 64, d.Nf * sizeof(cplx), ctx->stream>>>(ctx->s.Sigma, ctx->t.Ekg, ctx->t.tw_tau, ctx->s.scal,
-                                                               ctx->s.Grt_work, d.Nx, d.Ny, d.Nf, d.Ngrain,
-                                                               ctx->p.beta);
-  int rc = after_launch(ctx, "k_grt_points");
+                                                               out, d.Nx, d.Ny, d.Nf, d.Ngrain, ctx->p.beta);
+  return after_launch(ctx, "k_grt_points");
+}
+
+int launch_grt(tups_ctx* ctx) {
+  int rc = launch_grt_pre(ctx, ctx->s.Grt_work);
   if (rc) return rc;
   return launch_fft2d(ctx, ctx->s.Grt_work, ctx->s.Grt, 1);
 }
 
-int launch_fft2d(tups_ctx* ctx, const cplx* in, cplx* out, int forward) {
+int launch_fft2d_batch(tups_ctx* ctx, const cplx* in, cplx* out, int nslices, int forward) {
   const auto& d = ctx->d;
   const int n1 = d.Nx * d.Ngrain, n2 = d.Ny * d.Ngrain;
   size_t sm = 2 * (size_t)n1 * n2 * sizeof(cplx);
   if (sm > 200 * 1024) return set_error(ctx, TUPS_ERR_BADDIM, "fine k grid too large for the in-CTA DFT");
   if (sm > 48 * 1024) cudaFuncSetAttribute(k_fft2d, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  k_fft2d<<<d.Nf, 256, sm, ctx->stream>>>(in, out, ctx->t.tw_x, ctx->t.tw_y, n1, n2, forward);
+  k_fft2d<<<nslices, 256, sm, ctx->stream>>>(in, out, ctx->t.tw_x, ctx->t.tw_y, n1, n2, forward);
   return after_launch(ctx, "k_fft2d");
+}
+
+int launch_fft2d(tups_ctx* ctx, const cplx* in, cplx* out, int forward) {
+  return launch_fft2d_batch(ctx, in, out, ctx->d.Nf, forward);
 }
 
 int launch_gkw(tups_ctx* ctx) {

@@ -63,6 +63,24 @@ struct DeviceState {
   double* red = nullptr;      // reduction scratch
 };
 
+// buffers of the every-5-iterations readout, allocated on its first use
+struct ReadoutBufs {
+  bool ready = false;
+  double* sd = nullptr;     // FF_sdwave (Nx*Ny, 4), k = kx*Ny + ky
+  double* sd2 = nullptr;    // its square
+  cplx* pre = nullptr;      // pre-FFT G(k, tau) (n1, n2, Nf)
+  cplx* ffg_in = nullptr;   // 4 x (n1, n2, Nf)
+  cplx* ffg = nullptr;      // 4 x (n1, n2, Nf)
+  cplx* prod = nullptr;     // 10 x (n1, n2, Nf)
+  cplx* prod_ft = nullptr;  // 10 x (n1, n2, Nf)
+  cplx* chi0 = nullptr;     // 10 x (Nred): ph, pp, ph_FF[4], pp_FF[4]
+  cplx* chi0_bz = nullptr;  // 10 x (Nx*Ny*Nf/2)
+  cplx* gph = nullptr;      // (Nl*nbox, Nb, 4)
+  cplx* gpp = nullptr;
+  cplx* sus = nullptr;      // (Nb, 4 ff, 4 channels)
+  cplx* sus_bz = nullptr;   // 16 x (Nx*Ny*Nf/2)
+};
+
 // slots of DeviceState::scal
 enum Scal {
   S_MU = 0,         // chemical potential
@@ -95,6 +113,7 @@ struct tups_ctx {
   bool have_exp = false, have_M = false, have_phir = false, have_green = false;
   tups::DeviceTables t;
   tups::DeviceState s;
+  tups::ReadoutBufs rd;
   std::vector<void*> allocations;
   // instrumentation: event pairs per phase, reused across calls
   bool timing = false;
@@ -137,5 +156,8 @@ int launch_output_mu(tups_ctx* ctx);
 int launch_fft2d(tups_ctx* ctx, const cplx* in, cplx* out, int forward);
 int launch_chi_aux(tups_ctx* ctx);
 int launch_fill_lambda_block(tups_ctx* ctx, cplx* F, cplx* G, double value);
+int launch_grt_pre(tups_ctx* ctx, cplx* out);
+int launch_fft2d_batch(tups_ctx* ctx, const cplx* in, cplx* out, int nslices, int forward);
+int launch_readout(tups_ctx* ctx);
 
 }  // namespace tups

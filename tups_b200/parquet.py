@@ -251,6 +251,28 @@ class Solver:
     def synchronize(self) -> None:
         self._call("tups_synchronize")
 
+    # -- readout (loop.f90:181-213 without HDF5) --
+    def readout(self, ite: int = 0) -> None:
+        """calc_Gkw_Grt(.true.) + exact chi0 + calc_sus + symmetrize_sus."""
+        self._call("tups_readout", int(ite))
+
+    def chi0(self, bz: bool = False) -> dict:
+        n = self.Nc * (self.Nf // 2) if bz else self.Nred
+        out = {"chi0_ph": np.empty(n, dtype=np.complex128), "chi0_pp": np.empty(n, dtype=np.complex128),
+               "chi0_ph_FF": np.empty((n, 4), dtype=np.complex128, order="F"),
+               "chi0_pp_FF": np.empty((n, 4), dtype=np.complex128, order="F")}
+        self._call("tups_get_chi0", int(bool(bz)), *(_ptr(out[k]) for k in ("chi0_ph", "chi0_pp", "chi0_ph_FF",
+                                                                           "chi0_pp_FF")))
+        return out
+
+    def sus(self, channel, bz: bool = False) -> np.ndarray:
+        """sus_r_IBZ (Nred, 4) or, with bz, sus_r (Nx*Ny*Nf/2, 4)."""
+        ch = CHANNELS.index(channel) if isinstance(channel, str) else int(channel)
+        n = self.Nc * (self.Nf // 2) if bz else self.Nred
+        a = np.empty((n, 4), dtype=np.complex128, order="F")
+        self._call("tups_get_sus", ch, int(bool(bz)), _ptr(a))
+        return a
+
     # -- instrumentation --
     def set_timing(self, enable: bool) -> None:
         self._call("tups_set_timing", int(bool(enable)))
