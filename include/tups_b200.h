@@ -210,6 +210,22 @@ int tups_synchronize(tups_ctx* ctx);
 /* number of this library's kernels launched since context creation */
 long long tups_kernel_launches(const tups_ctx* ctx);
 
+/* ---- LU form of the BSE, batched over instances of uneven size -------------
+ * No counterpart in the reference (its BSE is the damped two-ordering update,
+ * SRC/parquet_BSE.f90:72-128, whose fixed point this reproduces):
+ *   F_i = (1 - scale_i Gamma_i chi_i)^{-1} Gamma_i   (want_phi: F_i - Gamma_i)
+ * for n_inst instances of size n[i] = nl[i] * Nnu_i, in one persistent launch
+ * (CTAs take instances largest first; partial-pivoting LU, panel 16, FP64
+ * tensor-core trailing updates; n[i] right-hand sides).  n, nl, scale: host
+ * arrays.  gamma, out, work: device, instances packed consecutively as
+ * (n, n) column-major complex128; chi: device, packed (nl, nl, Nnu) blocks;
+ * ipiv: device int, packed n[i].  status (host, optional): per instance 0, or
+ * k+1 when column k had a zero pivot; when given, the call synchronises.
+ * Allocates nothing; limit n_inst <= 16384. */
+int tups_bse_lu_batched(int n_inst, const int* n, const int* nl, const double* scale, const double* gamma,
+                        const double* chi, double* out, double* work, int* ipiv, int want_phi, int* status,
+                        void* stream);
+
 /* ---- BSE update without device allocation ----------------------------------
  * No counterpart in the reference.  For callers that may not allocate device
  * memory while they call this library (a host that gives all device memory

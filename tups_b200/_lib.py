@@ -94,6 +94,9 @@ _PROTOS = {
     "tups_get_tables": [C.c_void_p] + [C.c_void_p] * 7,
     "tups_get_sde_aux": [C.c_void_p] + [C.c_void_p] * 5,
     "tups_synchronize": [C.c_void_p],
+    "tups_bse_lu_batched": [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double), C.c_void_p,
+                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int),
+                            C.c_void_p],
     "tups_bse_noalloc": [C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
                          C.c_double, C.c_void_p],
     "tups_set_timing": [C.c_void_p, C.c_int],
