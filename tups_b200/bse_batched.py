@@ -127,9 +127,21 @@ def make_instances(n_q: int = 64, n_w: int = 16, nf: int = 64, Nx: int = 8, beta
         jobs.append((i, seed, int(nffs[i]), nf, Nx, beta, rho, qx, qy, w, FFs[int(nffs[i])]))
     if workers > 0:
         import multiprocessing as mp
+        import os
         from concurrent.futures import ProcessPoolExecutor
-        with ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
-            res = list(ex.map(_one_instance, jobs, chunksize=4))
+        # one BLAS thread per worker: the children inherit these at spawn
+        saved = {k: os.environ.get(k) for k in ("OPENBLAS_NUM_THREADS", "OMP_NUM_THREADS", "MKL_NUM_THREADS")}
+        for k in saved:
+            os.environ[k] = "1"
+        try:
+            with ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
+                res = list(ex.map(_one_instance, jobs, chunksize=1))
+        finally:
+            for k, v in saved.items():
+                if v is None:
+                    os.environ.pop(k, None)
+                else:
+                    os.environ[k] = v
     else:
         res = [_one_instance(j) for j in jobs]
     gam = [r[0] for r in res]
