@@ -166,6 +166,19 @@ int tups_iteration(tups_ctx* ctx, int ite, tups_conv_info* info);
  * *ite_out = iterations done */
 int tups_execute_loop(tups_ctx* ctx, int* ite_out, int* converged);
 
+/* ---- warm start and checkpoint ----------------------------------------------
+ * Warm start at the reference's initialisation hook (SRC/preprocessing.f90:100-116,
+ * SRC/parquet_util.f90:178-233): Sigma <- sigma (Nt complex, host); mu by
+ * bisection for it; Gamma_r <- gamma_l1[r] (4 complex, host) on the (l=1,l=1)
+ * nu-block and 0 elsewhere; F_r from ONE BSE solve in LU form,
+ * F_r = (1 - 2 c_r/(beta Nx Ny) Gamma_r chi_r)^{-1} Gamma_r, i.e. the fixed
+ * point of the reference's damped update for that Gamma_r.  Then continue
+ * with tups_iteration. */
+int tups_warm_start(tups_ctx* ctx, const double* sigma, const double* gamma_l1);
+/* device-side copy of the loop state (Sigma, SigmaOld, mu, F_r, G_r, previous
+ * vertex maxima): save = 1 stores it, save = 0 restores the stored copy */
+int tups_checkpoint(tups_ctx* ctx, int save);
+
 /* ---- readout (SRC/loop.f90:181-213 without HDF5) -------------------------- */
 /* calc_Gkw_Grt(ite, Grt, .true.) with the exact chi0 bubble
  * (SRC/parquet_chi.f90:216-430), calc_sus (SRC/parquet_sus.f90:18-643) and

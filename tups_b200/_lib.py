@@ -75,6 +75,8 @@ _PROTOS = {
     "tups_output_block": [C.c_void_p],
     "tups_iteration": [C.c_void_p, C.c_int, C.POINTER(tups_conv_info)],
     "tups_execute_loop": [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)],
+    "tups_warm_start": [C.c_void_p, C.c_void_p, C.c_void_p],
+    "tups_checkpoint": [C.c_void_p, C.c_int],
     "tups_readout": [C.c_void_p, C.c_int],
     "tups_get_chi0": [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
     "tups_get_sus": [C.c_void_p, C.c_int, C.c_int, C.c_void_p],

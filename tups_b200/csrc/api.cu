@@ -470,3 +470,80 @@ extern "C" int tups_synchronize(tups_ctx* ctx) {
   if (!ctx) return TUPS_ERR_BADARG;
   return tups::cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "synchronize");
 }
+
+// ---- warm start and checkpoint ----------------------------------------------
+static int dev_alloc(tups_ctx* ctx, void** p, size_t bytes, const char* what) {
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return tups::set_error(ctx, TUPS_ERR_OOM, what);
+  }
+  ctx->allocations.push_back(*p);
+  return TUPS_OK;
+}
+
+extern "C" int tups_warm_start(tups_ctx* ctx, const double* sigma, const double* gamma_l1) {
+  if (!ctx || !sigma || !gamma_l1) return TUPS_ERR_BADARG;
+  TRY(set_dev(ctx));
+  const auto& d = ctx->d;
+  const size_t n2b = (size_t)d.Nz * d.Nz * d.Nb;
+  if (!ctx->lu_work) {
+    TRY(dev_alloc(ctx, (void**)&ctx->lu_work, n2b * sizeof(cplx), "warm-start LU workspace"));
+    TRY(dev_alloc(ctx, (void**)&ctx->lu_ipiv, (size_t)d.Nz * d.Nb * sizeof(int), "warm-start pivots"));
+  }
+  TRY(copy_h2d(ctx, ctx->s.Sigma, sigma, (size_t)d.Nt * sizeof(cplx)));
+  TRY(green_async(ctx, 0));
+  TRY(tups::launch_chi(ctx, 0, d.Nb));
+  TRY(device_status(ctx));
+  const double a = 1.0 / (ctx->p.beta * d.Nx * d.Ny);
+  const double c[4] = {0.5, 0.5, -0.25, 0.25};
+  std::vector<int> n(d.Nb, d.Nz), nl(d.Nb, d.Nl), status(d.Nb, 0);
+  for (int r = 0; r < 4; r++) {
+    TRY(tups::launch_set_l1_block(ctx, ctx->s.G[r], gamma_l1[2 * r], gamma_l1[2 * r + 1]));
+    std::vector<double> scale(d.Nb, 2.0 * c[r] * a);
+    const tups::cplx* chi = r < 2 ? ctx->s.chi_ph : ctx->s.chi_pp;
+    int rc = tups_bse_lu_batched(d.Nb, n.data(), nl.data(), scale.data(), (const double*)ctx->s.G[r],
+                                 (const double*)chi, (double*)ctx->s.F[r], (double*)ctx->lu_work, ctx->lu_ipiv, 0,
+                                 status.data(), ctx->stream);
+    if (rc) return tups::set_error(ctx, rc, "warm-start BSE solve failed");
+    for (int q = 0; q < d.Nb; q++)
+      if (status[q]) return tups::set_error(ctx, TUPS_ERR_NAN, "warm-start BSE kernel singular");
+    ctx->launches++;
+  }
+  for (int r = 0; r < 4; r++) ctx->F_max_prev[r] = 0.0;
+  return tups::cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "warm start");
+}
+
+extern "C" int tups_checkpoint(tups_ctx* ctx, int save) {
+  if (!ctx) return TUPS_ERR_BADARG;
+  TRY(set_dev(ctx));
+  const auto& d = ctx->d;
+  const size_t vb = (size_t)d.Nz * d.Nz * d.Nb * sizeof(cplx), sb = (size_t)d.Nt * sizeof(cplx);
+  if (!ctx->ck_sigma) {
+    for (int r = 0; r < 4; r++) {
+      TRY(dev_alloc(ctx, (void**)&ctx->ck_F[r], vb, "checkpoint"));
+      TRY(dev_alloc(ctx, (void**)&ctx->ck_G[r], vb, "checkpoint"));
+    }
+    TRY(dev_alloc(ctx, (void**)&ctx->ck_sigma, sb, "checkpoint"));
+    TRY(dev_alloc(ctx, (void**)&ctx->ck_sigma_old, sb, "checkpoint"));
+  }
+  if (!save && !ctx->ck_valid) return tups::set_error(ctx, TUPS_ERR_STATE, "no checkpoint stored");
+  auto cp = [&](void* dst, const void* src, size_t b) {
+    return tups::cuda_check(ctx, cudaMemcpyAsync(dst, src, b, cudaMemcpyDeviceToDevice, ctx->stream), "checkpoint");
+  };
+  for (int r = 0; r < 4; r++) {
+    TRY(save ? cp(ctx->ck_F[r], ctx->s.F[r], vb) : cp(ctx->s.F[r], ctx->ck_F[r], vb));
+    TRY(save ? cp(ctx->ck_G[r], ctx->s.G[r], vb) : cp(ctx->s.G[r], ctx->ck_G[r], vb));
+  }
+  TRY(save ? cp(ctx->ck_sigma, ctx->s.Sigma, sb) : cp(ctx->s.Sigma, ctx->ck_sigma, sb));
+  TRY(save ? cp(ctx->ck_sigma_old, ctx->s.SigmaOld, sb) : cp(ctx->s.SigmaOld, ctx->ck_sigma_old, sb));
+  if (save) {
+    TRY(read_scalars(ctx, ctx->ck_scal));
+    for (int r = 0; r < 4; r++) ctx->ck_fmax[r] = ctx->F_max_prev[r];
+    ctx->ck_valid = true;
+  } else {
+    TRY(copy_h2d(ctx, ctx->s.scal, ctx->ck_scal, tups::S_COUNT * sizeof(double)));
+    for (int r = 0; r < 4; r++) ctx->F_max_prev[r] = ctx->ck_fmax[r];
+  }
+  return tups::cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "checkpoint");
+}

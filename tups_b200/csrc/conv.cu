@@ -96,6 +96,23 @@ int launch_fill_lambda_block(tups_ctx* ctx, cplx* F, cplx* G, double value) {
   return after_launch(ctx, "k_fill_lambda_block");
 }
 
+// G = 0 except value on the (l=1, l=1) nu-block of every slot
+__global__ void k_set_l1_block(cplx* __restrict__ G, int Nz, int Nf, int Nb, double vr, double vi) {
+  const size_t n = (size_t)Nz * Nz * Nb;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(e % Nz), j = (int)((e / Nz) % Nz);
+    G[e] = (i < Nf && j < Nf) ? cmk(vr, vi) : cmk(0.0, 0.0);
+  }
+}
+
+int launch_set_l1_block(tups_ctx* ctx, cplx* G, double vr, double vi) {
+  const auto& d = ctx->d;
+  const size_t n = (size_t)d.Nz * d.Nz * d.Nb;
+  k_set_l1_block<<<(unsigned)std::min<size_t>(cdiv(n, 256), 148 * 8), 256, 0, ctx->stream>>>(G, d.Nz, d.Nf, d.Nb, vr,
+                                                                                           vi);
+  return after_launch(ctx, "k_set_l1_block");
+}
+
 int launch_conv(tups_ctx* ctx) {
   const auto& d = ctx->d;
   k_conv_sigma<<<1, 1024, 0, ctx->stream>>>(ctx->s.Sigma, ctx->s.SigmaOld, ctx->s.scal, d.Nt);

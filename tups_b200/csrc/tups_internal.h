@@ -114,6 +114,16 @@ struct tups_ctx {
   tups::DeviceTables t;
   tups::DeviceState s;
   tups::ReadoutBufs rd;
+  // warm start (LU workspace) and checkpoint, allocated on first use
+  tups::cplx* lu_work = nullptr;
+  int* lu_ipiv = nullptr;
+  tups::cplx* ck_F[4] = {};
+  tups::cplx* ck_G[4] = {};
+  tups::cplx* ck_sigma = nullptr;
+  tups::cplx* ck_sigma_old = nullptr;
+  double ck_scal[16] = {};
+  double ck_fmax[4] = {};
+  bool ck_valid = false;
   std::vector<void*> allocations;
   // instrumentation: event pairs per phase, reused across calls
   bool timing = false;
@@ -159,5 +169,6 @@ int launch_fill_lambda_block(tups_ctx* ctx, cplx* F, cplx* G, double value);
 int launch_grt_pre(tups_ctx* ctx, cplx* out);
 int launch_fft2d_batch(tups_ctx* ctx, const cplx* in, cplx* out, int nslices, int forward);
 int launch_readout(tups_ctx* ctx);
+int launch_set_l1_block(tups_ctx* ctx, cplx* G, double vr, double vi);
 
 }  // namespace tups

@@ -251,6 +251,19 @@ class Solver:
     def synchronize(self) -> None:
         self._call("tups_synchronize")
 
+    # -- warm start and checkpoint --
+    def warm_start(self, sigma: np.ndarray, gamma_l1) -> None:
+        """Sigma <- sigma; mu by bisection; Gamma_r <- gamma_l1[r] on the (l=1, l=1)
+        nu-block; F_r <- (1 - 2 c_r/(beta Nx Ny) Gamma_r chi_r)^{-1} Gamma_r."""
+        sig = np.ascontiguousarray(sigma, dtype=np.complex128).reshape(-1)
+        assert sig.size == self.Nt
+        gam = np.ascontiguousarray(gamma_l1, dtype=np.complex128).reshape(4)
+        self._call("tups_warm_start", _ptr(sig), _ptr(gam))
+
+    def checkpoint(self, save: bool = True) -> None:
+        """Store (save) or restore the device-side loop state."""
+        self._call("tups_checkpoint", int(bool(save)))
+
     # -- readout (loop.f90:181-213 without HDF5) --
     def readout(self, ite: int = 0) -> None:
         """calc_Gkw_Grt(.true.) + exact chi0 + calc_sus + symmetrize_sus."""
