@@ -179,6 +179,30 @@ int tups_warm_start(tups_ctx* ctx, const double* sigma, const double* gamma_l1);
  * vertex maxima): save = 1 stores it, save = 0 restores the stored copy */
 int tups_checkpoint(tups_ctx* ctx, int save);
 
+/* ---- multilayer perceptron of the learned warm start ------------------------
+ * No counterpart in the reference.  FP32 network n_in -> n_hidden (x n_layers,
+ * SiLU) -> n_out (linear), trained by Adam on the mean squared error.  Flat
+ * parameters [W_0, b_0, W_1, b_1, ...], W_l (out, in) row-major.  Inputs,
+ * targets and outputs are HOST row-major (batch, features) float arrays. */
+typedef struct tups_mlp tups_mlp;
+int tups_mlp_create(int n_in, int n_hidden, int n_layers, int n_out, int max_batch, int device, tups_mlp** out);
+int tups_mlp_destroy(tups_mlp* m);
+const char* tups_mlp_last_error(const tups_mlp* m);
+long long tups_mlp_num_params(const tups_mlp* m);
+long long tups_mlp_kernel_launches(const tups_mlp* m);
+/* set_params also resets the optimiser state */
+int tups_mlp_set_params(tups_mlp* m, const float* host);
+int tups_mlp_get_params(tups_mlp* m, float* host);
+int tups_mlp_forward(tups_mlp* m, const float* x, int batch, float* y);
+/* loss (mean squared error) and its gradient w.r.t. the flat parameters;
+ * grad or loss may be NULL */
+int tups_mlp_gradients(tups_mlp* m, const float* x, const float* t, int batch, float* grad, double* loss);
+/* epochs of minibatch Adam (beta 0.9/0.999, eps 1e-8) over a resident copy of
+ * (x, t), shuffled per epoch from seed; decoupled weight decay on W only;
+ * loss_per_epoch (optional, host, epochs entries) = mean minibatch loss */
+int tups_mlp_train(tups_mlp* m, const float* x, const float* t, int n_samples, int batch, int epochs, float lr,
+                   float weight_decay, unsigned long long seed, double* loss_per_epoch);
+
 /* ---- readout (SRC/loop.f90:181-213 without HDF5) -------------------------- */
 /* calc_Gkw_Grt(ite, Grt, .true.) with the exact chi0 bubble
  * (SRC/parquet_chi.f90:216-430), calc_sus (SRC/parquet_sus.f90:18-643) and

@@ -102,6 +102,14 @@ _PROTOS = {
     "tups_bse_noalloc": [C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
                          C.c_double, C.c_void_p],
     "tups_set_timing": [C.c_void_p, C.c_int],
+    "tups_mlp_create": [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p)],
+    "tups_mlp_destroy": [C.c_void_p],
+    "tups_mlp_set_params": [C.c_void_p, C.c_void_p],
+    "tups_mlp_get_params": [C.c_void_p, C.c_void_p],
+    "tups_mlp_forward": [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p],
+    "tups_mlp_gradients": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_double)],
+    "tups_mlp_train": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float,
+                       C.c_ulonglong, C.c_void_p],
     "tups_get_phase_times": [C.c_void_p, C.c_void_p, C.c_void_p],
     "tups_record_event": [C.c_void_p, C.c_int],
     "tups_event_elapsed": [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double)],
@@ -112,6 +120,9 @@ _SPECIAL = {
     "tups_last_error": ([C.c_void_p], C.c_char_p),
     "tups_strerror": ([C.c_int], C.c_char_p),
     "tups_kernel_launches": ([C.c_void_p], C.c_longlong),
+    "tups_mlp_last_error": ([C.c_void_p], C.c_char_p),
+    "tups_mlp_num_params": ([C.c_void_p], C.c_longlong),
+    "tups_mlp_kernel_launches": ([C.c_void_p], C.c_longlong),
 }
 
 _lib = None
