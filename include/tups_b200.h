@@ -179,6 +179,25 @@ int tups_warm_start(tups_ctx* ctx, const double* sigma, const double* gamma_l1);
  * vertex maxima): save = 1 stores it, save = 0 restores the stored copy */
 int tups_checkpoint(tups_ctx* ctx, int save);
 
+/* ---- split-precision BSE and ZGEMM ---------------------------------------------
+ * No counterpart in the reference (its BSE GEMMs are FP64 ZGEMMs,
+ * SRC/parquet_BSE.f90:72-128).  The complex GEMM is emulated with int8
+ * slices on the tensor cores (tcgen05 kind::i8, exact int32 sums) and FP64
+ * recombination: relative error about 10^(1.1 - 2 s) of max|A| max|B| K
+ * for s slices per operand (s = 8: FP64 level).
+ * tups_set_bse_precision: slices = 0 keeps the FP64 tensor-core GEMM;
+ * 2..8 uses s slices in every BSE; ladder = 1 picks s per iteration from the
+ * last relative Sigma change (3 slices before the first, 8 at the end). */
+int tups_set_bse_precision(tups_ctx* ctx, int slices, int ladder);
+/* slices the next BSE will use (0 = FP64) */
+int tups_get_bse_slices(const tups_ctx* ctx);
+/* Batched C_b = A_b B_b: A (M, K), B (K, N), C (M, N) column-major complex128,
+ * batches packed contiguously, all DEVICE pointers; work: device buffer of
+ * tups_zgemm_split_workspace() bytes.  Synchronises the stream. */
+size_t tups_zgemm_split_workspace(int batch, int M, int N, int K, int slices);
+int tups_zgemm_split(int batch, int M, int N, int K, const double* A, const double* B, double* C, int slices,
+                     void* work, size_t work_bytes, void* stream);
+
 /* ---- multilayer perceptron of the learned warm start ------------------------
  * No counterpart in the reference.  FP32 network n_in -> n_hidden (x n_layers,
  * SiLU) -> n_out (linear), trained by Adam on the mean squared error.  Flat

@@ -1,0 +1,101 @@
+"""Split-precision GEMM (int8 tcgen05) on a B200 against the oracle's
+emulation and against FP64."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from oracle import split as S
+import parity
+
+pytestmark = pytest.mark.gpu
+
+# the GPU sums the same exact int32 diagonals as the oracle and adds them in
+# the same FP64 order: only the conversion of the final sums may differ
+EMU_TOL = 1e-15
+
+
+def _zgemm_split(lib, A, B, s):
+    import torch
+    batch, M, K = A.shape
+    N = B.shape[2]
+    # column-major per batch = A_b^T row-major
+    dA = torch.from_numpy(np.ascontiguousarray(A.transpose(0, 2, 1))).cuda()
+    dB = torch.from_numpy(np.ascontiguousarray(B.transpose(0, 2, 1))).cuda()
+    dC = torch.zeros((batch, N, M), dtype=torch.complex128, device="cuda")
+    ws = lib.tups_zgemm_split_workspace(batch, M, N, K, s)
+    assert ws > 0
+    work = torch.empty(ws, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    rc = lib.tups_zgemm_split(batch, M, N, K, C.c_void_p(dA.data_ptr()), C.c_void_p(dB.data_ptr()),
+                              C.c_void_p(dC.data_ptr()), s, C.c_void_p(work.data_ptr()), ws, C.c_void_p(stream))
+    assert rc == 0, rc
+    return dC.cpu().numpy().transpose(0, 2, 1)
+
+
+@pytest.mark.parametrize("dims", [(2, 128, 80, 64), (3, 200, 150, 300), (1, 40, 8, 7)],
+                         ids=["aligned", "ragged", "tiny"])
+@pytest.mark.parametrize("s", [2, 5, 8])
+def test_zgemm_split_matches_the_emulation(gpu_lib, dims, s):
+    batch, M, N, K = dims
+    rng = np.random.default_rng(M + N + K + s)
+    A = (rng.normal(size=(batch, M, K)) + 1j * rng.normal(size=(batch, M, K))) * np.logspace(-2, 2, K)[None, None, :]
+    B = rng.normal(size=(batch, K, N)) + 1j * rng.normal(size=(batch, K, N))
+    got = _zgemm_split(gpu_lib, A, B, s)
+    for b in range(batch):
+        emu = S.ozaki_zgemm(A[b], B[b], s)
+        assert parity.rel(got[b], emu) <= EMU_TOL, (b, parity.rel(got[b], emu))
+        exact = A[b] @ B[b]
+        assert parity.rel(got[b], exact) <= 10.0 ** (1.6 - 2.0 * s) + 1e-14
+
+
+def test_split_bse_against_fp64(gpu_lib):
+    from oracle import tups_oracle as O
+    from tups_b200 import Solver
+    p = O.Params(beta=3.0, U=2.0, nParticle=0.9, Nx=4, Nf=8, neighbours=2, tprime=-0.1, f_damping=0.5,
+                 ite_max=20)
+    sol = Solver(parity.to_solver_params(p))
+    for ite in range(3):
+        sol.iteration(ite)
+    sol.checkpoint(True)
+    sol.calc_Gkw_Grt(3)
+    sol.BSE(3)
+    ref = [sol.G(r) for r in range(4)]
+    for s, tol in ((8, 1e-13), (6, 1e-9), (4, 1e-5)):
+        sol.checkpoint(False)
+        sol.set_bse_precision(s)
+        assert sol.bse_slices == s
+        sol.calc_Gkw_Grt(3)
+        sol.BSE(3)
+        err = max(parity.rel(sol.G(r), ref[r]) for r in range(4))
+        assert err <= tol, (s, err)
+    sol.close()
+
+
+def test_ladder_loop_reaches_the_fp64_fixed_point(gpu_lib):
+    from tups_b200 import Params, Solver
+    p = Params(beta=3.0, U=2.0, nParticle=0.9, Nx=4, Nf=8, neighbours=2, tprime=-0.1, f_damping=0.5,
+               ite_max=10 ** 6, conv_abs=1e-10)
+    ref = Solver(p)
+    n_ref = 0
+    while not ref.iteration(n_ref)["converged"]:
+        n_ref += 1
+    n_ref += 1
+    sig_ref = ref.Sigma
+    ref.close()
+    sol = Solver(p)
+    sol.set_bse_precision(0, ladder=True)
+    used = []
+    n = 0
+    while True:
+        used.append(sol.bse_slices)
+        ci = sol.iteration(n)
+        n += 1
+        if ci["converged"]:
+            break
+        assert n < 3 * n_ref
+    assert used[0] == 3 and used[-1] >= 7
+    assert parity.rel(sol.Sigma, sig_ref) <= 1e-10 * 50   # 1e-10 absolute on |Sigma| ~ 0.1..1
+    sol.close()

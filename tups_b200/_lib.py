@@ -102,6 +102,9 @@ _PROTOS = {
     "tups_bse_noalloc": [C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
                          C.c_double, C.c_void_p],
     "tups_set_timing": [C.c_void_p, C.c_int],
+    "tups_set_bse_precision": [C.c_void_p, C.c_int, C.c_int],
+    "tups_zgemm_split": [C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                         C.c_void_p, C.c_size_t, C.c_void_p],
     "tups_mlp_create": [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p)],
     "tups_mlp_destroy": [C.c_void_p],
     "tups_mlp_set_params": [C.c_void_p, C.c_void_p],
@@ -121,6 +124,8 @@ _SPECIAL = {
     "tups_strerror": ([C.c_int], C.c_char_p),
     "tups_kernel_launches": ([C.c_void_p], C.c_longlong),
     "tups_mlp_last_error": ([C.c_void_p], C.c_char_p),
+    "tups_get_bse_slices": ([C.c_void_p], C.c_int),
+    "tups_zgemm_split_workspace": ([C.c_int, C.c_int, C.c_int, C.c_int, C.c_int], C.c_size_t),
     "tups_mlp_num_params": ([C.c_void_p], C.c_longlong),
     "tups_mlp_kernel_launches": ([C.c_void_p], C.c_longlong),
 }

@@ -211,6 +211,7 @@ extern "C" int tups_conv(tups_ctx* ctx, tups_conv_info* info) {
   }
   if (ctx->p.conv_abs > 0.0) ok = ci.dsigma_inf < ctx->p.conv_abs;
   ci.converged = ok ? 1 : 0;
+  ctx->last_dsigma_rel = sc[tups::S_SIGMAX] > 0.0 ? ci.dsigma_inf / sc[tups::S_SIGMAX] : -1.0;
   const size_t bytes = (size_t)ctx->d.Nt * sizeof(cplx);
   TRY(tups::cuda_check(ctx,
                        cudaMemcpyAsync(ctx->s.SigmaOld, ctx->s.Sigma, bytes, cudaMemcpyDeviceToDevice, ctx->stream),
@@ -547,3 +548,13 @@ extern "C" int tups_checkpoint(tups_ctx* ctx, int save) {
   }
   return tups::cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "checkpoint");
 }
+
+extern "C" int tups_set_bse_precision(tups_ctx* ctx, int slices, int ladder) {
+  if (!ctx) return TUPS_ERR_BADARG;
+  if (slices < 0 || slices > 8 || slices == 1) return tups::set_error(ctx, TUPS_ERR_BADARG, "slices must be 0 or 2..8");
+  ctx->bse_slices = slices;
+  ctx->precision_ladder = ladder != 0;
+  return TUPS_OK;
+}
+
+extern "C" int tups_get_bse_slices(const tups_ctx* ctx) { return ctx ? tups::current_bse_slices(ctx) : -1; }

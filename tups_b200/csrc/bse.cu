@@ -221,6 +221,83 @@ static int run_gemm(tups_ctx* ctx, const BsePtrs& P, int q_begin, int q_count) {
   return after_launch(ctx, "k_bse_gemm");
 }
 
+// slices of the split GEMM for this BSE call: fixed, or chosen from the last
+// relative Sigma change so that the GEMM error (about 10^(1.1 - 2 s) of
+// max|A| max|B| K) stays two decades below it; 0 = FP64 tensor cores
+int current_bse_slices(const tups_ctx* ctx) {
+  if (!ctx->precision_ladder) return ctx->bse_slices;
+  const double r = ctx->last_dsigma_rel;
+  if (r < 0.0) return 3;
+  if (r == 0.0) return 8;
+  const int s = (int)std::ceil((3.1 - std::log10(r)) / 2.0);
+  return std::max(2, std::min(8, s));
+}
+
+// Split-precision GEMM [Gamma chi | F] [F ; chi Gamma] for the chunk, in
+// sub-chunks that fit the int8 workspace; same epilogue as k_bse_gemm.
+static int run_split(tups_ctx* ctx, const BsePtrs& P, int q_begin, int q_count, int slices) {
+  const int Nz = ctx->d.Nz;
+  if (!ctx->oz_work) {
+    // workspace for up to 8 slices, bounded to 8 GiB
+    const size_t per = oz_work_layout(4, Nz, Nz, 2 * Nz, 8).total / 4 + 1;
+    size_t cap = ((size_t)8 << 30) / per;
+    cap = std::max<size_t>(4, std::min<size_t>(cap, ctx->s.bse_chunk)) / 4 * 4;
+    const size_t bytes = oz_work_layout((int)cap, Nz, Nz, 2 * Nz, 8).total;
+    cudaError_t e = cudaMalloc(&ctx->oz_work, bytes);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      ctx->oz_work = nullptr;
+      return set_error(ctx, TUPS_ERR_OOM, "split-precision BSE workspace");
+    }
+    ctx->allocations.push_back(ctx->oz_work);
+    ctx->oz_cap = cap;
+  }
+  const int n_inst = 4 * q_count;
+  for (int i0 = 0; i0 < n_inst; i0 += (int)ctx->oz_cap) {
+    const int nb = std::min<int>((int)ctx->oz_cap, n_inst - i0);
+    OzRun R;
+    R.batch = nb;
+    R.M = Nz;
+    R.N = Nz;
+    R.s = slices;
+    const int qb = q_begin + i0 / 4;
+    OzOperand A{}, B{};
+    A.p1 = ctx->s.bse_A + (size_t)Nz * Nz * i0;   // Gamma chi
+    A.s1 = (long long)Nz * Nz;
+    A.ld1 = Nz;
+    A.K1 = Nz;
+    A.bse2 = 1;                                    // F_r(q)
+    A.ld2 = Nz;
+    A.K2 = Nz;
+    B.bse1 = 1;                                    // F_r(q)
+    B.ld1 = Nz;
+    B.K1 = Nz;
+    B.p2 = ctx->s.bse_B + (size_t)Nz * Nz * i0;   // chi Gamma
+    B.s2 = (long long)Nz * Nz;
+    B.ld2 = Nz;
+    B.K2 = Nz;
+    for (int r = 0; r < 4; r++) A.F[r] = B.F[r] = P.F[r];
+    A.q_begin = B.q_begin = qb;
+    A.Nz = B.Nz = Nz;
+    R.A = A;
+    R.B = B;
+    oz_bind_work(R, oz_work_layout(nb, Nz, Nz, 2 * Nz, slices), ctx->oz_work);
+    R.status = ctx->s.scal + S_STATUS;
+    R.status_code = (double)TUPS_ERR_TIMEOUT;
+    R.epi = 1;
+    for (int r = 0; r < 4; r++) {
+      R.F[r] = P.F[r];
+      R.G[r] = P.G[r];
+      R.scale[r] = P.scale[r];
+    }
+    R.omf = 1.0 - ctx->p.f_damping;
+    R.q_begin = qb;
+    int rc = oz_run(R, ctx->stream, &ctx->launches);
+    if (rc) return set_error(ctx, rc, "split-precision BSE launch failed");
+  }
+  return TUPS_OK;
+}
+
 int launch_bse_chunk(tups_ctx* ctx, int q_begin, int q_count) {
   const auto& d = ctx->d;
   BsePtrs P;
@@ -240,6 +317,12 @@ int launch_bse_chunk(tups_ctx* ctx, int q_begin, int q_count) {
   phase_end(ctx, TUPS_PHASE_BSE_PREP);
   if (rc) return rc;
   phase_begin(ctx, TUPS_PHASE_BSE_GEMM);
+  const int slices = current_bse_slices(ctx);
+  if (slices > 0) {
+    rc = run_split(ctx, P, q_begin, q_count, slices);
+    phase_end(ctx, TUPS_PHASE_BSE_GEMM);
+    return rc;
+  }
   // tile choice: 64x64 when Nz is a multiple of 64 (or large), else 32x32
   if (d.Nz % 64 == 0 || d.Nz > 512) rc = run_gemm<64, 64, 16, 2, 2, 3>(ctx, P, q_begin, q_count);
   else if (d.Nz >= 32) rc = run_gemm<32, 32, 16, 2, 2, 3>(ctx, P, q_begin, q_count);

@@ -9,39 +9,45 @@ namespace tups {
 __global__ void __launch_bounds__(1024) k_conv_sigma(const cplx* __restrict__ S, const cplx* __restrict__ So,
                                                      double* scal, int Nt) {
   __shared__ double sh[32];
-  double mx = 0.0, sum = 0.0, dmx = 0.0, bad = 0.0;
+  double mx = 0.0, sum = 0.0, dmx = 0.0, bad = 0.0, smax = 0.0;
   for (int i = threadIdx.x; i < Nt; i += blockDim.x) {
     const cplx a = S[i], b = So[i];
     const double dx = b.x - a.x, dy = b.y - a.y;
     const double d = sqrt(dx * dx + dy * dy);
-    const double rel = d / sqrt(a.x * a.x + a.y * a.y);
+    const double as = sqrt(a.x * a.x + a.y * a.y);
+    const double rel = d / as;
     if (!isfinite(a.x) || !isfinite(a.y)) bad = 1.0;
     mx = fmax(mx, rel);
     dmx = fmax(dmx, d);
+    smax = fmax(smax, as);
     sum += rel;
   }
   mx = warp_max(mx);
   dmx = warp_max(dmx);
   bad = warp_max(bad);
-  __shared__ double smx[32], sdm[32], sbd[32];
+  smax = warp_max(smax);
+  __shared__ double smx[32], sdm[32], sbd[32], ssm[32];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   if (lane == 0) {
     smx[wid] = mx;
     sdm[wid] = dmx;
     sbd[wid] = bad;
+    ssm[wid] = smax;
   }
   sum = block_sum(sum, sh);
   if (threadIdx.x == 0) {
-    double a = 0.0, b = 0.0, c = 0.0;
+    double a = 0.0, b = 0.0, c = 0.0, e = 0.0;
     for (int w = 0; w < (int)(blockDim.x + 31) / 32; w++) {
       a = fmax(a, smx[w]);
       b = fmax(b, sdm[w]);
       c = fmax(c, sbd[w]);
+      e = fmax(e, ssm[w]);
     }
     scal[S_RELSIG] = a;
     scal[S_RELSIGAV] = fabs(sum / Nt);
     scal[S_DSIG] = b;
     scal[S_NANFLAG] = c;
+    scal[S_SIGMAX] = e;
     for (int r = 0; r < 4; r++) scal[S_FMAX + r] = 0.0;
   }
 }

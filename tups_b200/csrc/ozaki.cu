@@ -1,0 +1,702 @@
+// Split-precision complex GEMM on the int8 tensor cores (tcgen05.mma
+// kind::i8), used by the BSE in its split mode and exported as a batched
+// ZGEMM.  No counterpart in the reference (its BSE runs FP64 ZGEMMs,
+// SRC/parquet_BSE.f90:72-128).
+//
+// Error-free splitting after Ozaki, Ogita, Oishi & Rump (Numer. Algorithms
+// 59, 2012), with integer slices:
+//   C = A B (complex, M x K times K x N) is the real product C' = A' B' with
+//   A' = [Re A | Im A] (M x 2K) and B' whose column 2j is [Re B_j ; -Im B_j]
+//   and column 2j+1 is [Im B_j ; Re B_j].  Every row of A' is scaled by 2^-e
+//   (max |row| < 2^e) and cut into s int8 slices of 7 bits; every column of
+//   B' likewise.  Slice products with i + j = d < s are summed exactly in
+//   int32 on the tensor cores (|sum| <= s K' 127^2 < 2^31) and combined in
+//   FP64: C' = 2^(e+f) sum_d 2^(-7(d+2)) D_d.
+//
+// Layout: slices of A' as rows of Kpad bytes (K-major), slices of B' as rows
+// of Kpad bytes (one row per column of B'); Kpad = 2K rounded up to 128.
+// The GEMM kernel reads 128-byte K chunks of both with TMA (128-byte
+// swizzle), accumulates one diagonal d at a time in TMEM (two buffers, so
+// the FP64 drain of diagonal d overlaps the MMAs of diagonal d+1), and
+// folds each diagonal into an FP64 partial sum in global memory; the last
+// diagonal applies the scales and the caller's epilogue.
+#include <cuda.h>
+
+#include <algorithm>
+#include <cstring>
+
+#include "tups_device.cuh"
+
+namespace tups {
+
+constexpr int OZ_BM = 128;       // rows per tile (TMEM lanes)
+constexpr int OZ_BK = 128;       // K bytes per pipeline stage
+constexpr int OZ_STAGES = 4;
+constexpr int OZ_THREADS = 192;  // warps 0-3 drain, warp 4 MMA, warp 5 TMA
+constexpr int OZ_SLICE_BITS = 7;
+
+// ---- splitting ---------------------------------------------------------------
+// Operand: line = [X1 | X2] for rows of A, [Y1 ; Y2] for columns of B;
+// part 2 may be absent (K2 = 0).  Instance b of a batch uses X1 + b*s1,
+// X2 + b*s2, or, in BSE mode, the (q, r) vertex of the chunk.
+__device__ __forceinline__ const cplx* oz_part(const OzOperand& o, int part, int inst) {
+  const bool bse = part == 1 ? o.bse1 : o.bse2;
+  if (bse) {
+    const int q = o.q_begin + inst / 4, r = inst % 4;
+    return o.F[r] + (size_t)o.Nz * o.Nz * q;
+  }
+  return part == 1 ? o.p1 + (size_t)o.s1 * inst : o.p2 + (size_t)o.s2 * inst;
+}
+
+// s int8 slices of v * 2^-e into out[i * slice_stride], |v 2^-e| < 1
+__device__ __forceinline__ void oz_cut(double v, int e, int s, int8_t* out, size_t slice_stride) {
+  double r = ldexp(v, -e);
+  for (int i = 0; i < s; i++) {
+    const double x = r * 128.0;
+    const double a = trunc(x);
+    out[i * slice_stride] = (int8_t)(int)a;
+    r = x - a;
+  }
+}
+
+__device__ __forceinline__ int oz_exponent(double maxabs) {
+  int e = 0;
+  if (maxabs > 0.0) frexp(maxabs, &e);
+  return e;
+}
+
+// Rows of A': one CTA per 32 rows of one instance.  out: [inst][s][M][Kpad].
+__global__ void __launch_bounds__(256) k_oz_split_rows(OzOperand A, int M, int s, int Kpad, int8_t* __restrict__ out,
+                                                       double* __restrict__ rscale) {
+  const int inst = blockIdx.y;
+  const int m0 = blockIdx.x * 32;
+  const int Kc = A.K1 + A.K2;
+  const cplx* X1 = oz_part(A, 1, inst);
+  const cplx* X2 = A.K2 ? oz_part(A, 2, inst) : nullptr;
+  __shared__ double smax[8][33];
+  __shared__ int sexp[32];
+  __shared__ cplx tile[32][33];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  {
+    const int m = m0 + lane;
+    double mx = 0.0;
+    if (m < M)
+      for (int k = w; k < Kc; k += 8) {
+        const cplx v = k < A.K1 ? X1[m + (size_t)A.ld1 * k] : X2[m + (size_t)A.ld2 * (k - A.K1)];
+        mx = fmax(mx, fmax(fabs(v.x), fabs(v.y)));
+      }
+    smax[w][lane] = mx;
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double mx = 0.0;
+    for (int i = 0; i < 8; i++) mx = fmax(mx, smax[i][threadIdx.x]);
+    const int e = oz_exponent(mx);
+    sexp[threadIdx.x] = e;
+    const int m = m0 + threadIdx.x;
+    if (m < M) rscale[(size_t)inst * M + m] = ldexp(1.0, e);
+  }
+  __syncthreads();
+  const size_t slice_stride = (size_t)M * Kpad;
+  int8_t* base = out + (size_t)inst * s * slice_stride;
+  // thread -> (row, group of 4 columns): 8 groups x 32 rows
+  const int cg = threadIdx.x & 7, rr = threadIdx.x >> 3;
+  for (int k0 = 0; k0 < Kc; k0 += 32) {
+    // load a 32 x 32 tile, rows fastest
+    for (int e = threadIdx.x; e < 32 * 32; e += 256) {
+      const int r = e & 31, c = e >> 5;
+      const int m = m0 + r, k = k0 + c;
+      cplx v = cmk(0.0, 0.0);
+      if (m < M && k < Kc) v = k < A.K1 ? X1[m + (size_t)A.ld1 * k] : X2[m + (size_t)A.ld2 * (k - A.K1)];
+      tile[c][r] = v;
+    }
+    __syncthreads();
+    const int m = m0 + rr;
+    const int k = k0 + cg * 4;
+    if (m < M && k < Kc) {
+      const int e = sexp[rr];
+      int8_t re[4][8], im[4][8];
+      for (int c = 0; c < 4; c++) {
+        const cplx v = (k + c < Kc) ? tile[cg * 4 + c][rr] : cmk(0.0, 0.0);
+        oz_cut(v.x, e, s, &re[c][0], 1);
+        oz_cut(v.y, e, s, &im[c][0], 1);
+      }
+      int8_t* row = base + (size_t)m * Kpad;
+      for (int i = 0; i < s; i++) {
+        int8_t* dst = row + (size_t)i * slice_stride;
+        if ((Kc & 3) == 0 && k + 3 < Kc) {
+          *reinterpret_cast<char4*>(dst + k) = make_char4(re[0][i], re[1][i], re[2][i], re[3][i]);
+          *reinterpret_cast<char4*>(dst + Kc + k) = make_char4(im[0][i], im[1][i], im[2][i], im[3][i]);
+        } else {
+          for (int c = 0; c < 4 && k + c < Kc; c++) {
+            dst[k + c] = re[c][i];
+            dst[Kc + k + c] = im[c][i];
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+  // zero the K padding [2 Kc, Kpad) of this CTA's rows
+  const int pad = Kpad - 2 * Kc;
+  for (int e = threadIdx.x; e < 32 * pad * s; e += 256) {
+    const int b = e % pad, r = (e / pad) % 32, i = e / (pad * 32);
+    if (m0 + r < M) base[(size_t)i * slice_stride + (size_t)(m0 + r) * Kpad + 2 * Kc + b] = 0;
+  }
+}
+
+// Columns of B': one warp per complex column j of B (K1 + K2 long); writes
+// rows 2j and 2j+1 of every slice.  out: [inst][s][2N][Kpad].
+__global__ void __launch_bounds__(256) k_oz_split_cols(OzOperand B, int N, int s, int Kpad, int8_t* __restrict__ out,
+                                                       double* __restrict__ cscale) {
+  const int inst = blockIdx.y;
+  const int j = blockIdx.x * 8 + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (j >= N) return;
+  const int Kc = B.K1 + B.K2;
+  const cplx* Y1 = oz_part(B, 1, inst) + (size_t)B.ld1 * j;
+  const cplx* Y2 = B.K2 ? oz_part(B, 2, inst) + (size_t)B.ld2 * j : nullptr;
+  double mx = 0.0;
+  for (int k = lane; k < Kc; k += 32) {
+    const cplx v = k < B.K1 ? Y1[k] : Y2[k - B.K1];
+    mx = fmax(mx, fmax(fabs(v.x), fabs(v.y)));
+  }
+  mx = warp_max(mx);
+  const int e = oz_exponent(mx);
+  if (lane == 0) cscale[(size_t)inst * N + j] = ldexp(1.0, e);
+  const size_t slice_stride = (size_t)2 * N * Kpad;
+  int8_t* r0 = out + (size_t)inst * s * slice_stride + (size_t)(2 * j) * Kpad;
+  int8_t* r1 = r0 + Kpad;
+  for (int k = lane * 4; k < Kc; k += 128) {
+    int8_t re[4][8], im[4][8], nim[4][8];
+    for (int c = 0; c < 4; c++) {
+      const int kk = k + c;
+      const cplx v = kk < Kc ? (kk < B.K1 ? Y1[kk] : Y2[kk - B.K1]) : cmk(0.0, 0.0);
+      oz_cut(v.x, e, s, &re[c][0], 1);
+      oz_cut(v.y, e, s, &im[c][0], 1);
+      oz_cut(-v.y, e, s, &nim[c][0], 1);
+    }
+    for (int i = 0; i < s; i++) {
+      int8_t* d0 = r0 + (size_t)i * slice_stride;
+      int8_t* d1 = r1 + (size_t)i * slice_stride;
+      if ((Kc & 3) == 0 && k + 3 < Kc) {
+        *reinterpret_cast<char4*>(d0 + k) = make_char4(re[0][i], re[1][i], re[2][i], re[3][i]);
+        *reinterpret_cast<char4*>(d0 + Kc + k) = make_char4(nim[0][i], nim[1][i], nim[2][i], nim[3][i]);
+        *reinterpret_cast<char4*>(d1 + k) = make_char4(im[0][i], im[1][i], im[2][i], im[3][i]);
+        *reinterpret_cast<char4*>(d1 + Kc + k) = make_char4(re[0][i], re[1][i], re[2][i], re[3][i]);
+      } else {
+        for (int c = 0; c < 4 && k + c < Kc; c++) {
+          d0[k + c] = re[c][i];
+          d0[Kc + k + c] = nim[c][i];
+          d1[k + c] = im[c][i];
+          d1[Kc + k + c] = re[c][i];
+        }
+      }
+    }
+  }
+  // zero the K padding [2 Kc, Kpad) of rows 2j, 2j+1
+  for (int i = 0; i < s; i++)
+    for (int b = 2 * Kc + lane; b < Kpad; b += 32) {
+      r0[(size_t)i * slice_stride + b] = 0;
+      r1[(size_t)i * slice_stride + b] = 0;
+    }
+}
+
+// ---- tcgen05 helpers ------------------------------------------------------------
+__device__ __forceinline__ uint32_t oz_smem(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(oz_smem(bar)), "r"(count));
+}
+
+__device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(oz_smem(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// bounded wait: false when the CTA's abort flag is set (honor_abort) or
+// about 2 s pass, in which case the abort flag is set
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
+                                          bool honor_abort = true) {
+  const long long t0 = clock64();
+  for (uint32_t it = 0;; it++) {
+    if (mbar_try(bar, parity)) return true;
+    if ((it & 255) == 255) {
+      if (honor_abort && *abort_flag) return false;
+      if (clock64() - t0 > 4000000000LL) {
+        *abort_flag = 1;
+        return false;
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(oz_smem(bar)) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(oz_smem(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(oz_smem(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tc_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(oz_smem(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tc_mma_i8(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+__device__ __forceinline__ void tc_ld16(uint32_t taddr, int32_t* v) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15}, [%16];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+        "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// K-major operand tile with 128-byte swizzle: rows of 128 bytes, 8-row groups 1024 bytes apart
+__device__ __forceinline__ uint64_t oz_desc(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
+         ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+
+// ---- the GEMM ----------------------------------------------------------------------
+enum { OZ_EPI_ZGEMM = 0, OZ_EPI_BSE = 1 };
+
+struct OzGemm {
+  int M, N;            // complex output size; N' = 2N real columns
+  int s;               // slices
+  int kchunks;         // Kpad / 128
+  int n_tile;          // real columns per tile (multiple of 16, <= 256)
+  int m_tiles, n_tiles;
+  uint32_t tmem_cols;  // allocated TMEM columns (power of 2 >= 2 n_tile)
+  const double* rscale;  // [inst][M]
+  const double* cscale;  // [inst][N]
+  double* acc;           // [inst][2N][M] FP64 partial sums
+  double* status;        // set to status_code on a timed-out wait
+  double status_code;
+  int epi;
+  // OZ_EPI_ZGEMM: C (col-major M x N complex per instance)
+  cplx* C;
+  // OZ_EPI_BSE: Phi = scale[r] C + omf (F - G) written over G
+  cplx* F[4];
+  cplx* G[4];
+  double scale[4];
+  double omf;
+  int q_begin;
+};
+
+__global__ void __launch_bounds__(OZ_THREADS, 1)
+    k_oz_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, OzGemm P) {
+  extern __shared__ uint8_t oz_dyn[];
+  __shared__ uint64_t full_bar[OZ_STAGES], empty_bar[OZ_STAGES], accf_bar[2], acce_bar[2], done_bar;
+  __shared__ uint32_t tmem_base_sh;
+  __shared__ volatile int abort_sh;
+  __shared__ int issued_sh, consumed_sh;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int inst = blockIdx.y;
+  const int mt = blockIdx.x % P.m_tiles, nt = blockIdx.x / P.m_tiles;
+  const int m0 = mt * OZ_BM, n0 = nt * P.n_tile;
+  const int Np = 2 * P.N;
+  const uint32_t a_bytes = OZ_BM * OZ_BK, b_bytes = (uint32_t)P.n_tile * OZ_BK;
+  const uint32_t dyn = (oz_smem(oz_dyn) + 1023u) & ~1023u;
+  auto sA = [&](int st) { return dyn + (uint32_t)st * (a_bytes + b_bytes); };
+  auto sB = [&](int st) { return dyn + (uint32_t)st * (a_bytes + b_bytes) + a_bytes; };
+
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < OZ_STAGES; i++) {
+      mbar_init(&full_bar[i], 1);
+      mbar_init(&empty_bar[i], 1);
+    }
+    for (int i = 0; i < 2; i++) {
+      mbar_init(&accf_bar[i], 1);
+      mbar_init(&acce_bar[i], 4 * 32);
+    }
+    mbar_init(&done_bar, 1);
+    abort_sh = 0;
+    issued_sh = 0;
+    consumed_sh = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 4) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(oz_smem(&tmem_base_sh)),
+                 "r"(P.tmem_cols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_base_sh;
+  const uint32_t buf_cols = P.tmem_cols / 2;
+
+  if (warp == 5) {
+    // ---- TMA producer ----
+    if (lane == 0) {
+      int stage = 0;
+      uint32_t phase = 0;
+      int issued = 0;
+      bool ok = true;
+      for (int d = 0; d < P.s && ok; d++)
+        for (int i = 0; i <= d && ok; i++) {
+          const int j = d - i;
+          const int ya = (inst * P.s + i) * P.M + m0;
+          const int yb = (inst * P.s + j) * Np + n0;
+          for (int kc = 0; kc < P.kchunks; kc++) {
+            if (!mbar_wait(&empty_bar[stage], phase ^ 1u, &abort_sh)) {
+              ok = false;
+              break;
+            }
+            mbar_expect_tx(&full_bar[stage], a_bytes + b_bytes);
+            tma_load_2d(sA(stage), &tmA, kc * OZ_BK, ya, &full_bar[stage]);
+            tma_load_2d(sB(stage), &tmB, kc * OZ_BK, yb, &full_bar[stage]);
+            issued++;
+            if (++stage == OZ_STAGES) {
+              stage = 0;
+              phase ^= 1u;
+            }
+          }
+        }
+      issued_sh = issued;
+    }
+  } else if (warp == 4) {
+    // ---- MMA issuer ----
+    if (lane == 0) {
+      const uint32_t idesc = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(P.n_tile >> 3) << 17) |
+                             ((uint32_t)(OZ_BM >> 4) << 24);
+      int stage = 0;
+      uint32_t phase = 0;
+      int consumed = 0;
+      bool ok = true;
+      for (int d = 0; d < P.s && ok; d++) {
+        const int buf = d & 1;
+        if (d >= 2 && !mbar_wait(&acce_bar[buf], (uint32_t)((d - 2) >> 1) & 1u, &abort_sh)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t dtm = tmem + (uint32_t)buf * buf_cols;
+        uint32_t accum = 0;
+        for (int i = 0; i <= d && ok; i++)
+          for (int kc = 0; kc < P.kchunks; kc++) {
+            if (!mbar_wait(&full_bar[stage], phase, &abort_sh)) {
+              ok = false;
+              break;
+            }
+            consumed++;
+            tc_fence_after();
+            const uint64_t da = oz_desc(sA(stage)), db = oz_desc(sB(stage));
+#pragma unroll
+            for (int kk = 0; kk < OZ_BK / 32; kk++) {
+              tc_mma_i8(dtm, da + 2 * kk, db + 2 * kk, idesc, accum);
+              accum = 1;
+            }
+            tc_commit(&empty_bar[stage]);
+            if (++stage == OZ_STAGES) {
+              stage = 0;
+              phase ^= 1u;
+            }
+          }
+        if (ok) tc_commit(&accf_bar[buf]);
+      }
+      consumed_sh = consumed;
+      // every MMA issued by this thread has completed once done_bar flips
+      tc_commit(&done_bar);
+      mbar_wait(&done_bar, 0, &abort_sh, false);
+    }
+  } else {
+    // ---- drain: warps 0-3, thread = TMEM lane = row ----
+    const int row = warp * 32 + lane;
+    const int m = m0 + row;
+    const bool mok = m < P.M;
+    const size_t accb = (size_t)inst * Np;
+    int q = 0, r = 0;
+    const cplx *Fq = nullptr;
+    cplx* Gq = nullptr;
+    if (P.epi == OZ_EPI_BSE) {
+      q = P.q_begin + inst / 4;
+      r = inst % 4;
+      Fq = P.F[r] + (size_t)P.M * P.M * q;
+      Gq = P.G[r] + (size_t)P.M * P.M * q;
+    }
+    const double rs = mok ? P.rscale[(size_t)inst * P.M + m] : 0.0;
+    for (int d = 0; d < P.s; d++) {
+      const int buf = d & 1;
+      if (!mbar_wait(&accf_bar[buf], (uint32_t)(d >> 1) & 1u, &abort_sh)) break;
+      tc_fence_after();
+      const double w = ldexp(1.0, -OZ_SLICE_BITS * (d + 2));
+      const bool last = d == P.s - 1;
+      for (int c0 = 0; c0 < P.n_tile; c0 += 16) {
+        int32_t v[16];
+        tc_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)buf * buf_cols + (uint32_t)c0, v);
+        if (!mok) continue;
+#pragma unroll
+        for (int t = 0; t < 16; t += 2) {
+          const int np = n0 + c0 + t;  // even: real part of complex column np/2
+          if (np >= Np) break;
+          double* a0 = P.acc + (accb + np) * P.M + m;
+          double* a1 = a0 + P.M;
+          double x0 = __dmul_rn((double)v[t], w), x1 = __dmul_rn((double)v[t + 1], w);
+          if (d > 0) {
+            x0 = __dadd_rn(*a0, x0);
+            x1 = __dadd_rn(*a1, x1);
+          }
+          if (!last) {
+            *a0 = x0;
+            *a1 = x1;
+            continue;
+          }
+          const int jc = np >> 1;
+          const double sc = __dmul_rn(rs, P.cscale[(size_t)inst * P.N + jc]);
+          const double cre = __dmul_rn(x0, sc), cim = __dmul_rn(x1, sc);
+          if (P.epi == OZ_EPI_ZGEMM) {
+            P.C[(size_t)inst * P.M * P.N + m + (size_t)P.M * jc] = cmk(cre, cim);
+          } else {
+            const size_t idx = m + (size_t)P.M * jc;
+            const cplx f = Fq[idx], g = Gq[idx];
+            const double sr = P.scale[r];
+            Gq[idx] = cmk(__dadd_rn(__dmul_rn(sr, cre), __dmul_rn(P.omf, __dsub_rn(f.x, g.x))),
+                          __dadd_rn(__dmul_rn(sr, cim), __dmul_rn(P.omf, __dsub_rn(f.y, g.y))));
+          }
+        }
+      }
+      tc_fence_before();
+      mbar_arrive(&acce_bar[buf]);
+    }
+  }
+
+  __syncthreads();
+  if (threadIdx.x == 0 && abort_sh) {
+    *P.status = P.status_code;
+    // wait for the TMA copies that were issued but never consumed
+    int stage = consumed_sh % OZ_STAGES;
+    uint32_t phase = (uint32_t)(consumed_sh / OZ_STAGES) & 1u;
+    for (int k = consumed_sh; k < issued_sh; k++) {
+      mbar_wait(&full_bar[stage], phase, &abort_sh, false);
+      if (++stage == OZ_STAGES) {
+        stage = 0;
+        phase ^= 1u;
+      }
+    }
+  }
+  __syncthreads();
+  if (warp == 4) {
+    __syncwarp();
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(P.tmem_cols));
+  }
+}
+
+// ---- host side ----------------------------------------------------------------------
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+// 2-D byte tensor [rows][Kpad], boxes of 128 bytes x box_rows, 128-byte swizzle
+static bool make_map(CUtensorMap* map, const int8_t* base, long long rows, int Kpad, int box_rows) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return false;
+  if (((uintptr_t)base & 15) || (Kpad % OZ_BK) || box_rows < 1 || box_rows > 256) return false;
+  cuuint64_t dims[2] = {(cuuint64_t)Kpad, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)Kpad};
+  cuuint32_t box[2] = {(cuuint32_t)OZ_BK, (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  return fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, (void*)base, dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+int oz_kpad(int K) { return (int)(((long long)2 * K + OZ_BK - 1) / OZ_BK * OZ_BK); }
+
+// columns per tile: multiple of 16, <= 256; cost = tiles x (columns + 64),
+// the 64 standing for the per-tile cost of streaming the A rows
+int oz_n_tile(int N) {
+  const int Np = 2 * N;
+  int best = 16;
+  long long best_cost = -1;
+  for (int t = 16; t <= 256; t += 16) {
+    const long long cost = (long long)((Np + t - 1) / t) * (t + 64);
+    if (best_cost < 0 || cost < best_cost || (cost == best_cost && t > best)) {
+      best = t;
+      best_cost = cost;
+    }
+  }
+  return best;
+}
+
+size_t oz_smem_bytes(int n_tile) {
+  size_t s = (size_t)OZ_STAGES * (OZ_BM * OZ_BK + (size_t)n_tile * OZ_BK) + 1024;
+  return std::max<size_t>(s, 120 * 1024);  // one CTA per SM: the CTA owns its TMEM columns
+}
+
+OzWork oz_work_layout(int batch, int M, int N, int K, int s) {
+  OzWork w;
+  w.Kpad = oz_kpad(K);
+  w.a_bytes = (size_t)batch * s * M * w.Kpad;
+  w.b_bytes = (size_t)batch * s * 2 * N * w.Kpad;
+  w.rs_bytes = (size_t)batch * M * sizeof(double);
+  w.cs_bytes = (size_t)batch * N * sizeof(double);
+  w.acc_bytes = (size_t)batch * M * 2 * N * sizeof(double);
+  auto up = [](size_t x) { return (x + 255) / 256 * 256; };
+  w.total = up(w.a_bytes) + up(w.b_bytes) + up(w.rs_bytes) + up(w.cs_bytes) + up(w.acc_bytes) + 256;
+  return w;
+}
+
+void oz_bind_work(OzRun& R, const OzWork& w, void* base) {
+  auto up = [](size_t x) { return (x + 255) / 256 * 256; };
+  uint8_t* p = (uint8_t*)(((uintptr_t)base + 255) & ~(uintptr_t)255);
+  R.a_slices = (int8_t*)p;
+  p += up(w.a_bytes);
+  R.b_slices = (int8_t*)p;
+  p += up(w.b_bytes);
+  R.rscale = (double*)p;
+  p += up(w.rs_bytes);
+  R.cscale = (double*)p;
+  p += up(w.cs_bytes);
+  R.acc = (double*)p;
+}
+
+int oz_run(OzRun& R, cudaStream_t stream, long long* launches) {
+  const int M = R.M, N = R.N, s = R.s, batch = R.batch;
+  if (s < 1 || s > 8) return TUPS_ERR_BADARG;
+  if (R.A.K1 + R.A.K2 != R.B.K1 + R.B.K2) return TUPS_ERR_BADDIM;
+  const int K = R.A.K1 + R.A.K2;
+  // exactness of the int32 sums: s K' 127^2 < 2^31
+  if ((long long)s * 2 * K * 127 * 127 >= (1LL << 31)) return TUPS_ERR_BADDIM;
+  const int Kpad = oz_kpad(K);
+  if ((long long)batch * s * std::max(M, 2 * N) >= (1LL << 31)) return TUPS_ERR_BADDIM;
+  // rows of the split kernels
+  {
+    dim3 g((M + 31) / 32, batch);
+    k_oz_split_rows<<<g, 256, 0, stream>>>(R.A, M, s, Kpad, R.a_slices, R.rscale);
+    if (launches) (*launches)++;
+    dim3 gc((N + 7) / 8, batch);
+    k_oz_split_cols<<<gc, 256, 0, stream>>>(R.B, N, s, Kpad, R.b_slices, R.cscale);
+    if (launches) (*launches)++;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return TUPS_ERR_CUDA;
+  }
+  OzGemm P;
+  std::memset(&P, 0, sizeof(P));
+  P.M = M;
+  P.N = N;
+  P.s = s;
+  P.kchunks = Kpad / OZ_BK;
+  P.n_tile = oz_n_tile(N);
+  P.m_tiles = (M + OZ_BM - 1) / OZ_BM;
+  P.n_tiles = (2 * N + P.n_tile - 1) / P.n_tile;
+  uint32_t cols = 32;
+  while (cols < 2u * (uint32_t)P.n_tile) cols *= 2;
+  P.tmem_cols = cols;
+  P.rscale = R.rscale;
+  P.cscale = R.cscale;
+  P.acc = R.acc;
+  P.status = R.status;
+  P.status_code = R.status_code;
+  P.epi = R.epi;
+  P.C = R.C;
+  for (int r = 0; r < 4; r++) {
+    P.F[r] = R.F[r];
+    P.G[r] = R.G[r];
+    P.scale[r] = R.scale[r];
+  }
+  P.omf = R.omf;
+  P.q_begin = R.q_begin;
+  CUtensorMap ta, tb;
+  if (!make_map(&ta, R.a_slices, (long long)batch * s * M, Kpad, OZ_BM)) return TUPS_ERR_CUDA;
+  if (!make_map(&tb, R.b_slices, (long long)batch * s * 2 * N, Kpad, P.n_tile)) return TUPS_ERR_CUDA;
+  const size_t smem = oz_smem_bytes(P.n_tile);
+  cudaError_t e = cudaFuncSetAttribute(k_oz_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return TUPS_ERR_CUDA;
+  dim3 grid(P.m_tiles * P.n_tiles, batch);
+  k_oz_gemm<<<grid, OZ_THREADS, smem, stream>>>(ta, tb, P);
+  if (launches) (*launches)++;
+  e = cudaGetLastError();
+  return e == cudaSuccess ? TUPS_OK : TUPS_ERR_CUDA;
+}
+
+}  // namespace tups
+
+// ---- C-ABI: batched split-precision ZGEMM ---------------------------------------------
+extern "C" size_t tups_zgemm_split_workspace(int batch, int M, int N, int K, int slices) {
+  if (batch < 1 || M < 1 || N < 1 || K < 1 || slices < 1 || slices > 8) return 0;
+  return tups::oz_work_layout(batch, M, N, K, slices).total + 256;
+}
+
+extern "C" int tups_zgemm_split(int batch, int M, int N, int K, const double* A, const double* B, double* C,
+                                int slices, void* work, size_t work_bytes, void* stream) {
+  using namespace tups;
+  if (batch < 1 || M < 1 || N < 1 || K < 1 || !A || !B || !C || !work) return TUPS_ERR_BADARG;
+  if (slices < 1 || slices > 8) return TUPS_ERR_BADARG;
+  const OzWork w = oz_work_layout(batch, M, N, K, slices);
+  if (work_bytes < w.total + 256) return TUPS_ERR_BADARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  OzRun R;
+  R.batch = batch;
+  R.M = M;
+  R.N = N;
+  R.s = slices;
+  R.A.p1 = (const cplx*)A;
+  R.A.s1 = (long long)M * K;
+  R.A.ld1 = M;
+  R.A.K1 = K;
+  R.B.p1 = (const cplx*)B;
+  R.B.s1 = (long long)K * N;
+  R.B.ld1 = K;
+  R.B.K1 = K;
+  oz_bind_work(R, w, work);
+  // the status slot sits after the carved buffers
+  double* status = (double*)((uint8_t*)work + w.total);
+  status = (double*)(((uintptr_t)status + 7) & ~(uintptr_t)7);
+  if ((uint8_t*)(status + 1) > (uint8_t*)work + work_bytes) return TUPS_ERR_BADARG;
+  if (cudaMemsetAsync(status, 0, sizeof(double), st) != cudaSuccess) return TUPS_ERR_CUDA;
+  R.status = status;
+  R.status_code = 1.0;
+  R.epi = 0;
+  R.C = (cplx*)C;
+  int rc = oz_run(R, st, nullptr);
+  if (rc) return rc;
+  double flag = 0.0;
+  if (cudaMemcpyAsync(&flag, status, sizeof(double), cudaMemcpyDeviceToHost, st) != cudaSuccess) return TUPS_ERR_CUDA;
+  if (cudaStreamSynchronize(st) != cudaSuccess) return TUPS_ERR_CUDA;
+  return flag != 0.0 ? TUPS_ERR_TIMEOUT : TUPS_OK;
+}

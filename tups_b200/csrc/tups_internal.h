@@ -92,6 +92,7 @@ enum Scal {
   S_DSIG = 6,       // conv: max |dSigma|
   S_FMAX = 7,       // conv: max|F_r|, 4 slots (7..10)
   S_NANFLAG = 11,   // conv: NaN/Inf seen
+  S_SIGMAX = 12,    // conv: max |Sigma|
   S_COUNT = 16
 };
 
@@ -121,6 +122,13 @@ struct tups_ctx {
   tups::cplx* ck_G[4] = {};
   tups::cplx* ck_sigma = nullptr;
   tups::cplx* ck_sigma_old = nullptr;
+  // split-precision BSE: slices per operand (0 = FP64 tensor cores), the
+  // residual-driven ladder, and the int8 workspace (allocated on first use)
+  int bse_slices = 0;
+  bool precision_ladder = false;
+  double last_dsigma_rel = -1.0;
+  void* oz_work = nullptr;
+  size_t oz_cap = 0;           // instances per split sub-chunk
   double ck_scal[16] = {};
   double ck_fmax[4] = {};
   bool ck_valid = false;
@@ -144,6 +152,48 @@ void phase_collect(tups_ctx* ctx);
 
 namespace tups {
 
+// ---- split-precision (int8 slice) complex GEMM, ozaki.cu ----
+struct OzOperand {
+  const cplx* p1;
+  const cplx* p2;
+  long long s1, s2;   // element strides between instances (ignored for BSE parts)
+  int ld1, ld2;       // leading dimensions (column-major)
+  int K1, K2;         // complex lengths of the two parts along K
+  int bse2;           // 1: part 2 is F_r(q) of the BSE chunk (instance = 4 (q - q_begin) + r)
+  int bse1;           // 1: part 1 is F_r(q)
+  const cplx* F[4];
+  int q_begin, Nz;
+};
+
+struct OzWork {
+  int Kpad = 0;
+  size_t a_bytes = 0, b_bytes = 0, rs_bytes = 0, cs_bytes = 0, acc_bytes = 0, total = 0;
+};
+
+struct OzRun {
+  int batch = 0, M = 0, N = 0, s = 0;
+  OzOperand A{}, B{};
+  int8_t* a_slices = nullptr;
+  int8_t* b_slices = nullptr;
+  double* rscale = nullptr;
+  double* cscale = nullptr;
+  double* acc = nullptr;
+  double* status = nullptr;   // receives status_code when a wait times out
+  double status_code = 0.0;
+  int epi = 0;         // 0: C = A B; 1: BSE update written over G
+  cplx* C = nullptr;
+  cplx* F[4] = {};
+  cplx* G[4] = {};
+  double scale[4] = {};
+  double omf = 0.0;
+  int q_begin = 0;
+};
+
+OzWork oz_work_layout(int batch, int M, int N, int K, int s);
+// carve the workspace of oz_work_layout out of `base` into R
+void oz_bind_work(OzRun& R, const OzWork& w, void* base);
+int oz_run(OzRun& R, cudaStream_t stream, long long* launches);
+
 int set_error(tups_ctx* ctx, int code, const std::string& msg);
 int cuda_check(tups_ctx* ctx, cudaError_t e, const char* what);
 // record a kernel launch and check for launch errors
@@ -156,6 +206,7 @@ int launch_grt(tups_ctx* ctx);
 int launch_gkw(tups_ctx* ctx);
 int launch_chi(tups_ctx* ctx, int q_begin, int q_count);
 int launch_bse_chunk(tups_ctx* ctx, int q_begin, int q_count);
+int current_bse_slices(const tups_ctx* ctx);
 int launch_phir(tups_ctx* ctx);
 int launch_M(tups_ctx* ctx, int which);
 int launch_pae(tups_ctx* ctx);

@@ -251,6 +251,17 @@ class Solver:
     def synchronize(self) -> None:
         self._call("tups_synchronize")
 
+    # -- split-precision BSE --
+    def set_bse_precision(self, slices: int = 0, ladder: bool = False) -> None:
+        """slices = 0: FP64 tensor cores; 2..8: int8 slices per operand;
+        ladder: slices chosen per iteration from the last Sigma change."""
+        self._call("tups_set_bse_precision", int(slices), int(bool(ladder)))
+
+    @property
+    def bse_slices(self) -> int:
+        """Slices the next BSE uses (0 = FP64)."""
+        return int(self._lib.tups_get_bse_slices(self._ctx))
+
     # -- warm start and checkpoint --
     def warm_start(self, sigma: np.ndarray, gamma_l1) -> None:
         """Sigma <- sigma; mu by bisection; Gamma_r <- gamma_l1[r] on the (l=1, l=1)
