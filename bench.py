@@ -320,6 +320,12 @@ def run_tups(args, wl_name: str, wl: dict):
                 "unit": kd["unit"], "frac": kd["achieved"] / kd["peak"] if kd["peak"] else None,
                 "traffic": read_traffic(dom, wl_name), "peak_source": kd["peak_source"]}
     bse_tflops = kern.get("k_bse_gemm", {}).get("achieved")
+    split = None
+    conv = None
+    if not args.no_split:
+        split = split_iterations(params, device, K, W, Nz, Nb, peak64)
+        if Nz <= 256 and not args.no_convergence:
+            conv = to_convergence(params, device)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         sec = cpu_oracle_seconds_per_iteration(wl)
@@ -338,6 +344,8 @@ def run_tups(args, wl_name: str, wl: dict):
                            (8 * Nz * Nz * Nb * 16) / 1e9),
                        "parallelism": "replicas" if ws > 1 else "single GPU"},
             "bse_tflops": bse_tflops,
+            "split_precision": split,
+            "to_convergence": conv,
             "roofline": roof,
             "kernels": kern,
             "phase_ms_per_iter": {p: v[0] / K for p, v in phases.items()},
@@ -354,6 +362,77 @@ def run_tups(args, wl_name: str, wl: dict):
     if pg:
         pg.barrier()
         pg.destroy_process_group()
+
+
+SPLIT_SLICES = (3, 5, 7, 8)
+
+
+def split_iterations(params, device: int, K: int, W: int, Nz: int, Nb: int, peak64: float) -> dict:
+    """The same K iterations with the BSE GEMM on int8 slices (tcgen05 kind::i8):
+    device ms per iteration and per BSE GEMM phase for each slice count."""
+    from tups_b200 import Solver
+    out = {}
+    for s in SPLIT_SLICES:
+        sol = Solver(params, device=device)
+        sol.set_bse_precision(s)
+        for ite in range(W):
+            sol.iteration(ite)
+        sol.synchronize()
+        sol.set_timing(True)
+        sol.record_event(0)
+        for k in range(K):
+            sol.iteration(W + k)
+        sol.record_event(1)
+        ms = sol.event_elapsed_ms(0, 1) / K
+        ph = sol.phase_times()
+        sol.close()
+        gemm_ms = ph["bse_gemm"][0] / K
+        flops = 16.0 * Nz ** 3 * 4 * Nb
+        out[str(s)] = {"ms_per_iter": ms, "bse_gemm_ms": gemm_ms,
+                       "bse_effective_tflops": flops / (gemm_ms * 1e-3) / 1e12,
+                       "int8_tops": 2.0 * s * (s + 1) / 2 * Nz * (2 * Nz) * (4 * Nz) * 4 * Nb / (gemm_ms * 1e-3) / 1e12,
+                       "gemm_rel_err_model": 10.0 ** (1.1 - 2.0 * s)}
+    out["fp64_peak_tflops"] = peak64
+    out["note"] = ("effective TFLOP/s = FP64-equivalent 16 Nz^3 per (q, r) / split GEMM time; int8_tops = "
+                   "s(s+1)/2 slice products x 2 M (2N) (2K) / time")
+    return out
+
+
+def to_convergence(params, device: int, max_iter: int = 3000) -> dict:
+    """Wall time (device events around the host-driven loop) and iterations to
+    max|dSigma| < 1e-10 from the reference's initial state: FP64 BSE vs the
+    precision ladder; Sigma of the ladder run against the FP64 run."""
+    from dataclasses import replace
+    from tups_b200 import Solver
+    p = replace(params, conv_abs=1e-10, ite_max=10 ** 6)
+    res = {}
+    sig = {}
+    for name in ("fp64", "ladder"):
+        sol = Solver(p, device=device)
+        if name == "ladder":
+            sol.set_bse_precision(0, ladder=True)
+        used = []
+        sol.synchronize()
+        sol.record_event(4)
+        n, ok = 0, False
+        while n < max_iter:
+            used.append(sol.bse_slices)
+            ci = sol.iteration(n)
+            n += 1
+            if ci["converged"]:
+                ok = True
+                break
+        sol.record_event(5)
+        sec = sol.event_elapsed_ms(4, 5) * 1e-3
+        sig[name] = sol.Sigma
+        sol.close()
+        res[name] = {"iterations": n, "seconds": sec, "converged": ok}
+        if name == "ladder":
+            res[name]["slices_per_iteration"] = used
+    a, b = sig["ladder"], sig["fp64"]
+    res["sigma_rel_err_ladder_vs_fp64"] = float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+    res["speedup_ladder_vs_fp64"] = res["fp64"]["seconds"] / res["ladder"]["seconds"]
+    return res
 
 
 LU_WORKLOAD = "bse_lu_1024"
@@ -456,6 +535,8 @@ def main():
     ap.add_argument("--impl", choices=["tups", "reference"], default="tups")
     ap.add_argument("--workload", choices=sorted(WORKLOADS) + [LU_WORKLOAD], default=DEFAULT_WORKLOAD)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-split", action="store_true", help="skip the split-precision iterations")
+    ap.add_argument("--no-convergence", action="store_true", help="skip the runs to convergence")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "tups":
         args.warmup = 3

@@ -96,6 +96,25 @@ def test_ladder_loop_reaches_the_fp64_fixed_point(gpu_lib):
         if ci["converged"]:
             break
         assert n < 3 * n_ref
-    assert used[0] == 3 and used[-1] >= 7
+    # the tuner times FP64 on the first call and tries the split GEMM once
+    assert used[0] == 0 and any(u > 0 for u in used)
     assert parity.rel(sol.Sigma, sig_ref) <= 1e-10 * 50   # 1e-10 absolute on |Sigma| ~ 0.1..1
     sol.close()
+
+
+def test_fixed_slices_loop_reaches_the_fp64_fixed_point(gpu_lib):
+    from tups_b200 import Params, Solver
+    p = Params(beta=3.0, U=2.0, nParticle=0.9, Nx=4, Nf=8, neighbours=2, tprime=-0.1, f_damping=0.5,
+               ite_max=10 ** 6, conv_abs=1e-10)
+    sols = {}
+    for s in (0, 7):
+        sol = Solver(p)
+        sol.set_bse_precision(s)
+        n = 0
+        while not sol.iteration(n)["converged"]:
+            n += 1
+            assert n < 2000
+        sols[s] = sol.Sigma
+        sol.close()
+    # 7 slices: GEMM error ~1e-13 relative; the fixed points agree to 1e-10
+    assert parity.rel(sols[7], sols[0]) <= 1e-10

@@ -69,6 +69,13 @@ int green_async(tups_ctx* ctx, int cal_chi) {
 int bse_async(tups_ctx* ctx) {
   if (!ctx->have_green) return tups::set_error(ctx, TUPS_ERR_STATE, "BSE before calc_Gkw_Grt");
   const int Nb = ctx->d.Nb;
+  ctx->cur_slices = tups::current_bse_slices(ctx);
+  const bool tune = ctx->precision_ladder;
+  if (tune) {
+    for (int i = 0; i < 2; i++)
+      if (!ctx->tune_ev[i]) TRY(tups::cuda_check(ctx, cudaEventCreate(&ctx->tune_ev[i]), "event"));
+    TRY(tups::cuda_check(ctx, cudaEventRecord(ctx->tune_ev[0], ctx->stream), "event"));
+  }
   const int chunk_q = (int)std::max<size_t>(1, ctx->s.bse_chunk / 4);
   for (int q0 = 0; q0 < Nb; q0 += chunk_q) {
     const int nq = std::min(chunk_q, Nb - q0);
@@ -76,6 +83,10 @@ int bse_async(tups_ctx* ctx) {
     TRY(tups::launch_chi(ctx, q0, nq));
     tups::phase_end(ctx, TUPS_PHASE_CHI);
     TRY(tups::launch_bse_chunk(ctx, q0, nq));
+  }
+  if (tune) {
+    TRY(tups::cuda_check(ctx, cudaEventRecord(ctx->tune_ev[1], ctx->stream), "event"));
+    ctx->tune_pending = ctx->cur_slices;
   }
   return TUPS_OK;
 }
@@ -212,6 +223,7 @@ extern "C" int tups_conv(tups_ctx* ctx, tups_conv_info* info) {
   if (ctx->p.conv_abs > 0.0) ok = ci.dsigma_inf < ctx->p.conv_abs;
   ci.converged = ok ? 1 : 0;
   ctx->last_dsigma_rel = sc[tups::S_SIGMAX] > 0.0 ? ci.dsigma_inf / sc[tups::S_SIGMAX] : -1.0;
+  tups::bse_tune_collect(ctx);  // read_scalars synchronised the stream
   const size_t bytes = (size_t)ctx->d.Nt * sizeof(cplx);
   TRY(tups::cuda_check(ctx,
                        cudaMemcpyAsync(ctx->s.SigmaOld, ctx->s.Sigma, bytes, cudaMemcpyDeviceToDevice, ctx->stream),
@@ -554,6 +566,7 @@ extern "C" int tups_set_bse_precision(tups_ctx* ctx, int slices, int ladder) {
   if (slices < 0 || slices > 8 || slices == 1) return tups::set_error(ctx, TUPS_ERR_BADARG, "slices must be 0 or 2..8");
   ctx->bse_slices = slices;
   ctx->precision_ladder = ladder != 0;
+  ctx->cur_slices = slices;
   return TUPS_OK;
 }
 

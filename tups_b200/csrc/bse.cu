@@ -221,16 +221,43 @@ static int run_gemm(tups_ctx* ctx, const BsePtrs& P, int q_begin, int q_count) {
   return after_launch(ctx, "k_bse_gemm");
 }
 
-// slices of the split GEMM for this BSE call: fixed, or chosen from the last
-// relative Sigma change so that the GEMM error (about 10^(1.1 - 2 s) of
-// max|A| max|B| K) stays two decades below it; 0 = FP64 tensor cores
+// Slices of the split GEMM for the next BSE call; 0 = FP64 tensor cores.
+// Fixed mode: bse_slices.  Ladder: the accuracy needed is chosen from the last
+// relative Sigma change r so that the GEMM error (about 10^(1.1 - 2 s) of
+// max|A| max|B| K) stays two decades below it, s_req = ceil((3.1 - log10 r)/2)
+// (3 before the first conv); the online tuner then takes the faster of FP64
+// and s_req slices, from device times of earlier BSE calls.  Split times not
+// measured yet are predicted from a measured one in proportion to the
+// s (s + 1) / 2 slice products; FP64 is timed on the first call.
 int current_bse_slices(const tups_ctx* ctx) {
   if (!ctx->precision_ladder) return ctx->bse_slices;
   const double r = ctx->last_dsigma_rel;
-  if (r < 0.0) return 3;
-  if (r == 0.0) return 8;
-  const int s = (int)std::ceil((3.1 - std::log10(r)) / 2.0);
-  return std::max(2, std::min(8, s));
+  int s_req = 3;
+  if (r == 0.0) s_req = 9;
+  else if (r > 0.0) s_req = std::max(2, (int)std::ceil((3.1 - std::log10(r)) / 2.0));
+  if (s_req > 8) return 0;
+  if (ctx->tune_ms[0] < 0.0) return 0;
+  double est = ctx->tune_ms[s_req];
+  if (est < 0.0) {
+    int s0 = -1;
+    for (int s = 2; s <= 8; s++)
+      if (ctx->tune_ms[s] >= 0.0 && (s0 < 0 || std::abs(s - s_req) < std::abs(s0 - s_req))) s0 = s;
+    if (s0 < 0) return s_req;  // nothing measured yet: try it
+    est = ctx->tune_ms[s0] * (double)(s_req * (s_req + 1)) / (double)(s0 * (s0 + 1));
+  }
+  return est < ctx->tune_ms[0] ? s_req : 0;
+}
+
+void bse_tune_collect(tups_ctx* ctx) {
+  if (ctx->tune_pending < 0) return;
+  float ms = 0.0f;
+  if (cudaEventElapsedTime(&ms, ctx->tune_ev[0], ctx->tune_ev[1]) == cudaSuccess) {
+    double& slot = ctx->tune_ms[ctx->tune_pending];
+    slot = slot < 0.0 ? ms : 0.5 * (slot + ms);
+  } else {
+    cudaGetLastError();
+  }
+  ctx->tune_pending = -1;
 }
 
 // Split-precision GEMM [Gamma chi | F] [F ; chi Gamma] for the chunk, in
@@ -317,7 +344,7 @@ int launch_bse_chunk(tups_ctx* ctx, int q_begin, int q_count) {
   phase_end(ctx, TUPS_PHASE_BSE_PREP);
   if (rc) return rc;
   phase_begin(ctx, TUPS_PHASE_BSE_GEMM);
-  const int slices = current_bse_slices(ctx);
+  const int slices = ctx->cur_slices;
   if (slices > 0) {
     rc = run_split(ctx, P, q_begin, q_count, slices);
     phase_end(ctx, TUPS_PHASE_BSE_GEMM);

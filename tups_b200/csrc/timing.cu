@@ -54,6 +54,11 @@ void destroy_events(tups_ctx* ctx) {
       cudaEventDestroy(m);
       m = nullptr;
     }
+  for (auto& m : ctx->tune_ev)
+    if (m) {
+      cudaEventDestroy(m);
+      m = nullptr;
+    }
 }
 
 }  // namespace tups

@@ -129,6 +129,12 @@ struct tups_ctx {
   double last_dsigma_rel = -1.0;
   void* oz_work = nullptr;
   size_t oz_cap = 0;           // instances per split sub-chunk
+  // slices of the BSE in flight, and the online tuner of the ladder: device
+  // milliseconds of a whole BSE call (chi, prep, GEMM) per choice
+  int cur_slices = 0;
+  int tune_pending = -1;       // choice whose timing events are in flight
+  cudaEvent_t tune_ev[2] = {nullptr, nullptr};
+  double tune_ms[9] = {-1, -1, -1, -1, -1, -1, -1, -1, -1};  // [0] FP64, [s] s slices
   double ck_scal[16] = {};
   double ck_fmax[4] = {};
   bool ck_valid = false;
@@ -206,7 +212,10 @@ int launch_grt(tups_ctx* ctx);
 int launch_gkw(tups_ctx* ctx);
 int launch_chi(tups_ctx* ctx, int q_begin, int q_count);
 int launch_bse_chunk(tups_ctx* ctx, int q_begin, int q_count);
+// slices the next BSE call will use (0 = FP64), see bse.cu
 int current_bse_slices(const tups_ctx* ctx);
+// fold a finished BSE timing into the tuner (after the stream synchronised)
+void bse_tune_collect(tups_ctx* ctx);
 int launch_phir(tups_ctx* ctx);
 int launch_M(tups_ctx* ctx, int which);
 int launch_pae(tups_ctx* ctx);
