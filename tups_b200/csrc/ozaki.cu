@@ -31,8 +31,7 @@ namespace tups {
 
 constexpr int OZ_BM = 128;       // rows per tile (TMEM lanes)
 constexpr int OZ_BK = 128;       // K bytes per pipeline stage
-constexpr int OZ_STAGES = 4;
-constexpr int OZ_THREADS = 192;  // warps 0-3 drain, warp 4 MMA, warp 5 TMA
+constexpr int OZ_STAGES = 6;     // 6 x (16 KB of A + <= 16 KB of B) in flight
 constexpr int OZ_SLICE_BITS = 7;
 
 // ---- splitting ---------------------------------------------------------------
@@ -288,57 +287,71 @@ __device__ __forceinline__ uint64_t oz_desc(uint32_t saddr) {
 }
 
 // ---- the GEMM ----------------------------------------------------------------------
+// Persistent: each CTA walks tiles blockIdx.x, blockIdx.x + gridDim.x, ... of
+// the list (instance, row tile, column tile), instance outermost.  Per tile
+// and diagonal d the MMA warp accumulates the slice products (i, d - i) over
+// K into one of OZ_NBUF TMEM buffers; the eight drain warps (two per TMEM
+// lane quarter, each owning half of the tile's columns) fold the finished
+// buffer into FP64 registers, acc += 2^(-7(d+2)) D_d, while the MMAs of the
+// next diagonals proceed; after the last diagonal they apply the row and
+// column scales and the epilogue, and the next tile starts.
 enum { OZ_EPI_ZGEMM = 0, OZ_EPI_BSE = 1 };
+
+constexpr int OZ_NBUF = 4;            // TMEM accumulator buffers
+constexpr int OZ_MAX_NT = 128;        // columns per tile
+constexpr int OZ_HALF = OZ_MAX_NT / 2;
+constexpr int OZ_DRAIN_WARPS = 8;
+constexpr int OZ_THREADS2 = (OZ_DRAIN_WARPS + 2) * 32;  // + MMA warp + TMA warp
 
 struct OzGemm {
   int M, N;            // complex output size; N' = 2N real columns
   int s;               // slices
   int kchunks;         // Kpad / 128
-  int n_tile;          // real columns per tile (multiple of 16, <= 256)
-  int m_tiles, n_tiles;
-  uint32_t tmem_cols;  // allocated TMEM columns (power of 2 >= 2 n_tile)
+  int n_tile;          // real columns per tile (multiple of 16, <= 128)
+  int m_tiles, n_tiles, tiles;
   const double* rscale;  // [inst][M]
   const double* cscale;  // [inst][N]
-  double* acc;           // [inst][2N][M] FP64 partial sums
   double* status;        // set to status_code on a timed-out wait
   double status_code;
   int epi;
-  // OZ_EPI_ZGEMM: C (col-major M x N complex per instance)
-  cplx* C;
-  // OZ_EPI_BSE: Phi = scale[r] C + omf (F - G) written over G
-  cplx* F[4];
+  cplx* C;               // OZ_EPI_ZGEMM: col-major M x N per instance
+  cplx* F[4];            // OZ_EPI_BSE: Phi = scale[r] C + omf (F - G) over G
   cplx* G[4];
   double scale[4];
   double omf;
   int q_begin;
 };
 
-__global__ void __launch_bounds__(OZ_THREADS, 1)
+__device__ __forceinline__ void tc_ld8(uint32_t taddr, int32_t* v) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+               : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+               : "r"(taddr));
+}
+
+__global__ void __launch_bounds__(OZ_THREADS2, 1)
     k_oz_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, OzGemm P) {
   extern __shared__ uint8_t oz_dyn[];
-  __shared__ uint64_t full_bar[OZ_STAGES], empty_bar[OZ_STAGES], accf_bar[2], acce_bar[2], done_bar;
+  __shared__ uint64_t full_bar[OZ_STAGES], empty_bar[OZ_STAGES], accf_bar[OZ_NBUF], acce_bar[OZ_NBUF], done_bar;
   __shared__ uint32_t tmem_base_sh;
   __shared__ volatile int abort_sh;
   __shared__ int issued_sh, consumed_sh;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int inst = blockIdx.y;
-  const int mt = blockIdx.x % P.m_tiles, nt = blockIdx.x / P.m_tiles;
-  const int m0 = mt * OZ_BM, n0 = nt * P.n_tile;
   const int Np = 2 * P.N;
   const uint32_t a_bytes = OZ_BM * OZ_BK, b_bytes = (uint32_t)P.n_tile * OZ_BK;
   const uint32_t dyn = (oz_smem(oz_dyn) + 1023u) & ~1023u;
   auto sA = [&](int st) { return dyn + (uint32_t)st * (a_bytes + b_bytes); };
   auto sB = [&](int st) { return dyn + (uint32_t)st * (a_bytes + b_bytes) + a_bytes; };
+  const int per_inst = P.m_tiles * P.n_tiles;
 
   if (threadIdx.x == 0) {
     for (int i = 0; i < OZ_STAGES; i++) {
       mbar_init(&full_bar[i], 1);
       mbar_init(&empty_bar[i], 1);
     }
-    for (int i = 0; i < 2; i++) {
+    for (int i = 0; i < OZ_NBUF; i++) {
       mbar_init(&accf_bar[i], 1);
-      mbar_init(&acce_bar[i], 4 * 32);
+      mbar_init(&acce_bar[i], OZ_DRAIN_WARPS * 32);
     }
     mbar_init(&done_bar, 1);
     abort_sh = 0;
@@ -346,47 +359,49 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
     consumed_sh = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == 4) {
+  if (warp == OZ_DRAIN_WARPS) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(oz_smem(&tmem_base_sh)),
-                 "r"(P.tmem_cols));
+                 "r"(512u));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = tmem_base_sh;
-  const uint32_t buf_cols = P.tmem_cols / 2;
 
-  if (warp == 5) {
+  if (warp == OZ_DRAIN_WARPS + 1) {
     // ---- TMA producer ----
     if (lane == 0) {
       int stage = 0;
       uint32_t phase = 0;
       int issued = 0;
       bool ok = true;
-      for (int d = 0; d < P.s && ok; d++)
-        for (int i = 0; i <= d && ok; i++) {
-          const int j = d - i;
-          const int ya = (inst * P.s + i) * P.M + m0;
-          const int yb = (inst * P.s + j) * Np + n0;
-          for (int kc = 0; kc < P.kchunks; kc++) {
-            if (!mbar_wait(&empty_bar[stage], phase ^ 1u, &abort_sh)) {
-              ok = false;
-              break;
-            }
-            mbar_expect_tx(&full_bar[stage], a_bytes + b_bytes);
-            tma_load_2d(sA(stage), &tmA, kc * OZ_BK, ya, &full_bar[stage]);
-            tma_load_2d(sB(stage), &tmB, kc * OZ_BK, yb, &full_bar[stage]);
-            issued++;
-            if (++stage == OZ_STAGES) {
-              stage = 0;
-              phase ^= 1u;
+      for (int t = blockIdx.x; t < P.tiles && ok; t += gridDim.x) {
+        const int inst = t / per_inst, rem = t % per_inst;
+        const int m0 = (rem % P.m_tiles) * OZ_BM, n0 = (rem / P.m_tiles) * P.n_tile;
+        for (int d = 0; d < P.s && ok; d++)
+          for (int i = 0; i <= d && ok; i++) {
+            const int ya = (inst * P.s + i) * P.M + m0;
+            const int yb = (inst * P.s + (d - i)) * Np + n0;
+            for (int kc = 0; kc < P.kchunks; kc++) {
+              if (!mbar_wait(&empty_bar[stage], phase ^ 1u, &abort_sh)) {
+                ok = false;
+                break;
+              }
+              mbar_expect_tx(&full_bar[stage], a_bytes + b_bytes);
+              tma_load_2d(sA(stage), &tmA, kc * OZ_BK, ya, &full_bar[stage]);
+              tma_load_2d(sB(stage), &tmB, kc * OZ_BK, yb, &full_bar[stage]);
+              issued++;
+              if (++stage == OZ_STAGES) {
+                stage = 0;
+                phase ^= 1u;
+              }
             }
           }
-        }
+      }
       issued_sh = issued;
     }
-  } else if (warp == 4) {
+  } else if (warp == OZ_DRAIN_WARPS) {
     // ---- MMA issuer ----
     if (lane == 0) {
       const uint32_t idesc = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(P.n_tile >> 3) << 17) |
@@ -394,92 +409,110 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
       int stage = 0;
       uint32_t phase = 0;
       int consumed = 0;
+      int nacc = 0;  // accumulations issued so far (one per tile and diagonal)
       bool ok = true;
-      for (int d = 0; d < P.s && ok; d++) {
-        const int buf = d & 1;
-        if (d >= 2 && !mbar_wait(&acce_bar[buf], (uint32_t)((d - 2) >> 1) & 1u, &abort_sh)) {
-          ok = false;
-          break;
-        }
-        tc_fence_after();
-        const uint32_t dtm = tmem + (uint32_t)buf * buf_cols;
-        uint32_t accum = 0;
-        for (int i = 0; i <= d && ok; i++)
-          for (int kc = 0; kc < P.kchunks; kc++) {
-            if (!mbar_wait(&full_bar[stage], phase, &abort_sh)) {
-              ok = false;
-              break;
-            }
-            consumed++;
-            tc_fence_after();
-            const uint64_t da = oz_desc(sA(stage)), db = oz_desc(sB(stage));
-#pragma unroll
-            for (int kk = 0; kk < OZ_BK / 32; kk++) {
-              tc_mma_i8(dtm, da + 2 * kk, db + 2 * kk, idesc, accum);
-              accum = 1;
-            }
-            tc_commit(&empty_bar[stage]);
-            if (++stage == OZ_STAGES) {
-              stage = 0;
-              phase ^= 1u;
-            }
+      for (int t = blockIdx.x; t < P.tiles && ok; t += gridDim.x)
+        for (int d = 0; d < P.s && ok; d++, nacc++) {
+          const int buf = nacc % OZ_NBUF;
+          if (nacc >= OZ_NBUF &&
+              !mbar_wait(&acce_bar[buf], (uint32_t)((nacc - OZ_NBUF) / OZ_NBUF) & 1u, &abort_sh)) {
+            ok = false;
+            break;
           }
-        if (ok) tc_commit(&accf_bar[buf]);
-      }
+          tc_fence_after();
+          const uint32_t dtm = tmem + (uint32_t)(buf * OZ_MAX_NT);
+          uint32_t accum = 0;
+          for (int i = 0; i <= d && ok; i++)
+            for (int kc = 0; kc < P.kchunks; kc++) {
+              if (!mbar_wait(&full_bar[stage], phase, &abort_sh)) {
+                ok = false;
+                break;
+              }
+              consumed++;
+              tc_fence_after();
+              const uint64_t da = oz_desc(sA(stage)), db = oz_desc(sB(stage));
+#pragma unroll
+              for (int kk = 0; kk < OZ_BK / 32; kk++) {
+                tc_mma_i8(dtm, da + 2 * kk, db + 2 * kk, idesc, accum);
+                accum = 1;
+              }
+              tc_commit(&empty_bar[stage]);
+              if (++stage == OZ_STAGES) {
+                stage = 0;
+                phase ^= 1u;
+              }
+            }
+          if (ok) tc_commit(&accf_bar[buf]);
+        }
       consumed_sh = consumed;
-      // every MMA issued by this thread has completed once done_bar flips
       tc_commit(&done_bar);
       mbar_wait(&done_bar, 0, &abort_sh, false);
     }
   } else {
-    // ---- drain: warps 0-3, thread = TMEM lane = row ----
-    const int row = warp * 32 + lane;
-    const int m = m0 + row;
-    const bool mok = m < P.M;
-    const size_t accb = (size_t)inst * Np;
-    int q = 0, r = 0;
-    const cplx *Fq = nullptr;
-    cplx* Gq = nullptr;
-    if (P.epi == OZ_EPI_BSE) {
-      q = P.q_begin + inst / 4;
-      r = inst % 4;
-      Fq = P.F[r] + (size_t)P.M * P.M * q;
-      Gq = P.G[r] + (size_t)P.M * P.M * q;
-    }
-    const double rs = mok ? P.rscale[(size_t)inst * P.M + m] : 0.0;
-    for (int d = 0; d < P.s; d++) {
-      const int buf = d & 1;
-      if (!mbar_wait(&accf_bar[buf], (uint32_t)(d >> 1) & 1u, &abort_sh)) break;
-      tc_fence_after();
-      const double w = ldexp(1.0, -OZ_SLICE_BITS * (d + 2));
-      const bool last = d == P.s - 1;
-      for (int c0 = 0; c0 < P.n_tile; c0 += 16) {
-        int32_t v[16];
-        tc_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)buf * buf_cols + (uint32_t)c0, v);
-        if (!mok) continue;
+    // ---- drain: warp w reads TMEM lanes 32 (w % 4) .. + 31 and columns
+    //      [h n_tile/2, (h+1) n_tile/2), h = w / 4 ----
+    const int quarter = warp & 3, h = warp >> 2;
+    const int half = P.n_tile >> 1;
+    const int row = quarter * 32 + lane;
+    double acc[OZ_HALF];
+    int nacc = 0;
+    bool ok = true;
+    for (int t = blockIdx.x; t < P.tiles && ok; t += gridDim.x) {
+      const int inst = t / per_inst, rem = t % per_inst;
+      const int m0 = (rem % P.m_tiles) * OZ_BM, n0 = (rem / P.m_tiles) * P.n_tile;
+      const int m = m0 + row;
+      const bool mok = m < P.M;
 #pragma unroll
-        for (int t = 0; t < 16; t += 2) {
-          const int np = n0 + c0 + t;  // even: real part of complex column np/2
-          if (np >= Np) break;
-          double* a0 = P.acc + (accb + np) * P.M + m;
-          double* a1 = a0 + P.M;
-          double x0 = __dmul_rn((double)v[t], w), x1 = __dmul_rn((double)v[t + 1], w);
-          if (d > 0) {
-            x0 = __dadd_rn(*a0, x0);
-            x1 = __dadd_rn(*a1, x1);
+      for (int c = 0; c < OZ_HALF; c++) acc[c] = 0.0;
+      for (int d = 0; d < P.s; d++, nacc++) {
+        const int buf = nacc % OZ_NBUF;
+        if (!mbar_wait(&accf_bar[buf], (uint32_t)(nacc / OZ_NBUF) & 1u, &abort_sh)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const double w = ldexp(1.0, -OZ_SLICE_BITS * (d + 2));
+        const uint32_t tb = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(buf * OZ_MAX_NT + h * half);
+#pragma unroll
+        for (int c = 0; c < OZ_HALF; c += 8) {
+          if (c < half) {
+            int32_t v[8];
+            tc_ld8(tb + (uint32_t)c, v);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int e = 0; e < 8; e++) acc[c + e] = fma((double)v[e], w, acc[c + e]);
           }
-          if (!last) {
-            *a0 = x0;
-            *a1 = x1;
-            continue;
-          }
+        }
+        tc_fence_before();
+        mbar_arrive(&acce_bar[buf]);
+      }
+      if (!ok) break;
+      if (!mok) continue;
+      // scales and the epilogue; complex column jc = (n0 + h half + c) / 2
+      const double rs = P.rscale[(size_t)inst * P.M + m];
+      cplx* Cq = nullptr;
+      const cplx* Fq = nullptr;
+      cplx* Gq = nullptr;
+      int r = 0;
+      if (P.epi == OZ_EPI_BSE) {
+        const int q = P.q_begin + inst / 4;
+        r = inst % 4;
+        Fq = P.F[r] + (size_t)P.M * P.M * q;
+        Gq = P.G[r] + (size_t)P.M * P.M * q;
+      } else {
+        Cq = P.C + (size_t)inst * P.M * P.N;
+      }
+#pragma unroll
+      for (int c = 0; c < OZ_HALF; c += 2) {
+        const int np = n0 + h * half + c;
+        if (c < half && np < Np) {
           const int jc = np >> 1;
-          const double sc = __dmul_rn(rs, P.cscale[(size_t)inst * P.N + jc]);
-          const double cre = __dmul_rn(x0, sc), cim = __dmul_rn(x1, sc);
+          const double sc = rs * P.cscale[(size_t)inst * P.N + jc];
+          const double cre = acc[c] * sc, cim = acc[c + 1] * sc;
+          const size_t idx = m + (size_t)P.M * jc;
           if (P.epi == OZ_EPI_ZGEMM) {
-            P.C[(size_t)inst * P.M * P.N + m + (size_t)P.M * jc] = cmk(cre, cim);
+            Cq[idx] = cmk(cre, cim);
           } else {
-            const size_t idx = m + (size_t)P.M * jc;
             const cplx f = Fq[idx], g = Gq[idx];
             const double sr = P.scale[r];
             Gq[idx] = cmk(__dadd_rn(__dmul_rn(sr, cre), __dmul_rn(P.omf, __dsub_rn(f.x, g.x))),
@@ -487,8 +520,6 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
           }
         }
       }
-      tc_fence_before();
-      mbar_arrive(&acce_bar[buf]);
     }
   }
 
@@ -507,10 +538,10 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
     }
   }
   __syncthreads();
-  if (warp == 4) {
+  if (warp == OZ_DRAIN_WARPS) {
     __syncwarp();
     tc_fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(P.tmem_cols));
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512u));
   }
 }
 
@@ -547,13 +578,13 @@ static bool make_map(CUtensorMap* map, const int8_t* base, long long rows, int K
 
 int oz_kpad(int K) { return (int)(((long long)2 * K + OZ_BK - 1) / OZ_BK * OZ_BK); }
 
-// columns per tile: multiple of 16, <= 256; cost = tiles x (columns + 64),
+// columns per tile: multiple of 16, <= 128; cost = tiles x (columns + 64),
 // the 64 standing for the per-tile cost of streaming the A rows
 int oz_n_tile(int N) {
   const int Np = 2 * N;
   int best = 16;
   long long best_cost = -1;
-  for (int t = 16; t <= 256; t += 16) {
+  for (int t = 16; t <= OZ_MAX_NT; t += 16) {
     const long long cost = (long long)((Np + t - 1) / t) * (t + 64);
     if (best_cost < 0 || cost < best_cost || (cost == best_cost && t > best)) {
       best = t;
@@ -565,7 +596,7 @@ int oz_n_tile(int N) {
 
 size_t oz_smem_bytes(int n_tile) {
   size_t s = (size_t)OZ_STAGES * (OZ_BM * OZ_BK + (size_t)n_tile * OZ_BK) + 1024;
-  return std::max<size_t>(s, 120 * 1024);  // one CTA per SM: the CTA owns its TMEM columns
+  return std::max<size_t>(s, 120 * 1024);  // one CTA per SM: the CTA owns all 512 TMEM columns
 }
 
 OzWork oz_work_layout(int batch, int M, int N, int K, int s) {
@@ -575,7 +606,7 @@ OzWork oz_work_layout(int batch, int M, int N, int K, int s) {
   w.b_bytes = (size_t)batch * s * 2 * N * w.Kpad;
   w.rs_bytes = (size_t)batch * M * sizeof(double);
   w.cs_bytes = (size_t)batch * N * sizeof(double);
-  w.acc_bytes = (size_t)batch * M * 2 * N * sizeof(double);
+  w.acc_bytes = 0;  // the FP64 sums live in registers
   auto up = [](size_t x) { return (x + 255) / 256 * 256; };
   w.total = up(w.a_bytes) + up(w.b_bytes) + up(w.rs_bytes) + up(w.cs_bytes) + up(w.acc_bytes) + 256;
   return w;
@@ -591,8 +622,7 @@ void oz_bind_work(OzRun& R, const OzWork& w, void* base) {
   R.rscale = (double*)p;
   p += up(w.rs_bytes);
   R.cscale = (double*)p;
-  p += up(w.cs_bytes);
-  R.acc = (double*)p;
+  R.acc = nullptr;
 }
 
 int oz_run(OzRun& R, cudaStream_t stream, long long* launches) {
@@ -624,12 +654,10 @@ int oz_run(OzRun& R, cudaStream_t stream, long long* launches) {
   P.n_tile = oz_n_tile(N);
   P.m_tiles = (M + OZ_BM - 1) / OZ_BM;
   P.n_tiles = (2 * N + P.n_tile - 1) / P.n_tile;
-  uint32_t cols = 32;
-  while (cols < 2u * (uint32_t)P.n_tile) cols *= 2;
-  P.tmem_cols = cols;
+  if ((long long)batch * P.m_tiles * P.n_tiles >= (1LL << 31)) return TUPS_ERR_BADDIM;
+  P.tiles = batch * P.m_tiles * P.n_tiles;
   P.rscale = R.rscale;
   P.cscale = R.cscale;
-  P.acc = R.acc;
   P.status = R.status;
   P.status_code = R.status_code;
   P.epi = R.epi;
@@ -647,8 +675,11 @@ int oz_run(OzRun& R, cudaStream_t stream, long long* launches) {
   const size_t smem = oz_smem_bytes(P.n_tile);
   cudaError_t e = cudaFuncSetAttribute(k_oz_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return TUPS_ERR_CUDA;
-  dim3 grid(P.m_tiles * P.n_tiles, batch);
-  k_oz_gemm<<<grid, OZ_THREADS, smem, stream>>>(ta, tb, P);
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int grid = std::max(1, std::min(P.tiles, sms));
+  k_oz_gemm<<<grid, OZ_THREADS2, smem, stream>>>(ta, tb, P);
   if (launches) (*launches)++;
   e = cudaGetLastError();
   return e == cudaSuccess ? TUPS_OK : TUPS_ERR_CUDA;

@@ -427,6 +427,66 @@ def sweep(base: Params, runs: int = 200, n_train: int = 160, seed: int = 0, max_
                 loss=[float(v) for v in hist])
 
 
+def restart_study(params: Params, max_iter: int = 2000, device: int = 0) -> dict:
+    """How much an ideal warm start could save: converge cold, then restart
+    from the state after N_PLAIN plain iterations with parts of it replaced by
+    the converged ones (Sigma only, vertices only, both on the (l=1, l=1)
+    block only, everything), or moved a fraction a of the way back from the
+    converged state towards the 2-iteration state.  Returns iterations to
+    conv_abs per variant (N_PLAIN included)."""
+    sol = Solver(params, device=device)
+    n_cold = 0
+    while n_cold < max_iter and not sol.iteration(n_cold)["converged"]:
+        n_cold += 1
+    n_cold += 1
+    S = sol.Sigma
+    F = [sol.F(r) for r in range(4)]
+    G = [sol.G(r) for r in range(4)]
+    sol.close()
+    Nf = params.Nf
+    sol = Solver(params, device=device)
+    for ite in range(N_PLAIN):
+        sol.iteration(ite)
+    S2 = sol.Sigma
+    F2 = [sol.F(r) for r in range(4)]
+    G2 = [sol.G(r) for r in range(4)]
+    sol.checkpoint(True)
+
+    def put(sig, f, g):
+        sol.Sigma = sig
+        for r in range(4):
+            sol.set_vertex(r, 0, f[r])
+            sol.set_vertex(r, 1, g[r])
+
+    def l1(conv, two):
+        out = [x.copy() for x in two]
+        for r in range(4):
+            out[r][:Nf, :Nf] = conv[r][:Nf, :Nf]
+        return out
+
+    variants = {
+        "plain": None,
+        "sigma_converged": (S, F2, G2),
+        "vertices_converged": (S2, F, G),
+        "sigma_and_l1_block_converged": (S, l1(F, F2), l1(G, G2)),
+        "all_converged": (S, F, G),
+    }
+    for a in (0.01, 0.1, 0.5):
+        variants[f"converged+{a}*(2-iteration - converged)"] = (
+            S + a * (S2 - S), [x + a * (y - x) for x, y in zip(F, F2)], [x + a * (y - x) for x, y in zip(G, G2)])
+    out = {"cold_iterations": n_cold}
+    for name, st in variants.items():
+        sol.checkpoint(False)
+        if st is not None:
+            put(*st)
+        n = N_PLAIN
+        while n < max_iter and not sol.iteration(n)["converged"]:
+            n += 1
+        out[name] = n + 1
+    sol.close()
+    return out
+
+
 def main(argv=None) -> None:
     import argparse
     import json
@@ -441,9 +501,21 @@ def main(argv=None) -> None:
     ap.add_argument("--epochs", type=int, default=3000)
     ap.add_argument("--conv-abs", type=float, default=1e-10)
     ap.add_argument("--out", default=None, help="JSON file for the summary and per-run records")
+    ap.add_argument("--restart-study", action="store_true",
+                    help="only the ideal-restart study at U=2, beta=5, n=1 and U=3.5, beta=8, n=0.85, t'=-0.2")
     a = ap.parse_args(argv)
     base = Params(Nx=a.Nx, Nf=a.Nf, neighbours=a.neighbours, f_damping=0.5, use_U2=True, ite_max=10 ** 6,
                   conv_abs=a.conv_abs)
+    if a.restart_study:
+        res = {}
+        for kw in (dict(U=2.0, beta=5.0, nParticle=1.0, tprime=0.0),
+                   dict(U=3.5, beta=8.0, nParticle=0.85, tprime=-0.2)):
+            res[json.dumps(kw)] = restart_study(replace(base, **kw), max_iter=a.max_iter)
+            print(json.dumps({"params": kw, **res[json.dumps(kw)]}), flush=True)
+        if a.out:
+            with open(a.out, "w") as f:
+                json.dump(res, f, indent=1)
+        return
     res = sweep(base, runs=a.runs, n_train=a.train, seed=a.seed, max_iter=a.max_iter, epochs=a.epochs)
     print(json.dumps(res["summary"]))
     if a.out:
