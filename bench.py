@@ -238,6 +238,8 @@ def run_tups(args, wl_name: str, wl: dict):
     peak64 = fp64_peak_tflops(device)
     params = Params(**{k: v for k, v in wl.items() if k in Params.__dataclass_fields__})
     sol = Solver(params, device=device)
+    if args.bse_slices:
+        sol.set_bse_precision(args.bse_slices)
     K, W = args.steps, args.warmup
     for ite in range(W):
         sol.iteration(ite)
@@ -336,7 +338,8 @@ def run_tups(args, wl_name: str, wl: dict):
         line = {
             "metric": METRIC, "metric_full": METRIC_FULL, "value": value, "unit": "s/iter", "n_gpus": ws,
             "steps": K, "warmup": W, "ms_per_step": ms / K, "higher_is_better": False, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "vs_baseline": None, "dtype": "f64" if not args.bse_slices else f"f64 + int8x{args.bse_slices} BSE GEMM",
+            "data": "synthetic",
             "config": {"workload": wl_name,
                        **{k: wl[k] for k in ("Nx", "Nf", "neighbours", "beta", "U", "nParticle")},
                        "tprime": wl.get("tprime", 0.0), "Nl": d["Nl"], "Nz": Nz, "Nred": d["Nred"], "NR": NR,
@@ -536,6 +539,8 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS) + [LU_WORKLOAD], default=DEFAULT_WORKLOAD)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-split", action="store_true", help="skip the split-precision iterations")
+    ap.add_argument("--bse-slices", type=int, default=0,
+                    help="BSE GEMM of the main timed region on this many int8 slices (0 = FP64)")
     ap.add_argument("--no-convergence", action="store_true", help="skip the runs to convergence")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "tups":

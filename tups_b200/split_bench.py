@@ -34,13 +34,19 @@ def run(Nz: int, batch: int, slices, reps: int = 5, device: int = 0, check: bool
     e1 = torch.cuda.Event(enable_timing=True)
     At, Bt = A.transpose(1, 2), B.transpose(1, 2)
     ref = torch.matmul(At, Bt)
-    torch.cuda.synchronize()
-    e0.record()
-    for _ in range(reps):
-        torch.matmul(At, Bt)
-    e1.record()
-    torch.cuda.synchronize()
-    zgemm_ms = e0.elapsed_time(e1) / reps
+
+    def time_cublas() -> float:
+        for _ in range(3):
+            torch.matmul(At, Bt)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(reps):
+            torch.matmul(At, Bt)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    zgemm_ms = time_cublas()
     flops = 8.0 * M * N * K * batch
     out = []
     for s in slices:
@@ -69,6 +75,13 @@ def run(Nz: int, batch: int, slices, reps: int = 5, device: int = 0, check: bool
                 "speedup_vs_cublas": zgemm_ms / ms, "rel_err_vs_fp64": err}
         out.append(line)
         del work
+    # cuBLAS again after the split runs; keep its faster time
+    z2 = time_cublas()
+    if z2 < zgemm_ms:
+        for line in out:
+            line["cublas_zgemm_ms"] = z2
+            line["cublas_zgemm_tflops"] = flops / z2 / 1e9
+            line["speedup_vs_cublas"] = z2 / line["ms"]
     return out
 
 
@@ -79,7 +92,8 @@ def main(argv=None) -> None:
     ap.add_argument("--slices", type=int, nargs="+", default=[2, 3, 4, 5, 6, 7, 8])
     ap.add_argument("--reps", type=int, default=5)
     a = ap.parse_args(argv)
-    for line in run(a.Nz, a.batch, a.slices, a.reps):
+    lines = run(a.Nz, a.batch, a.slices, a.reps)
+    for line in lines:
         print(json.dumps(line), flush=True)
 
 
