@@ -111,37 +111,56 @@ __device__ __forceinline__ void dmma_16x8x8(double* c, const double* a, const do
       : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
 
-constexpr int PAE_E = 32;          // elements per CTA: an 8 (nu1) x 4 (nu2) block
-constexpr int PAE_TX = 8, PAE_TY = 4;
+constexpr int PAE_E = 32;          // listed elements per CTA
 constexpr int PAE_ROWS = 2 * PAE_E;  // (target, element) rows
 constexpr int PAE_BK = 16;
 constexpr int PAE_LDA = PAE_ROWS + 2;
 constexpr int PAE_LDB = PAE_BK + 4;
 
-// One CTA per (tile of 32 (nu1,nu2) elements, target pair x column chunk, q).
-// Warps: 4 along rows (16 rows each) x WN along the (l1,l2) columns, TN n8
-// tiles each; BN = 8 TN WN >= Nl^2 (or a chunk of it).
+// Element lists: for target pair p, family f and bosonic index W the
+// elements (nu1, nu2) the family reaches, packed as int4
+// {nu1 + 256 nu2, w2, a, b + 65536 tr}; capacity Nf^2 per list.
+__host__ __device__ __forceinline__ int pae_list(int pair, int fam, int W, int nh) {
+  return (pair * 2 + fam) * nh + (W - 1);
+}
+
+// F_r = Phi_r + Lambda_r * aux on the (l=1, l=1) block, all r and slots
+__global__ void k_pae_base(PaePtrs P, const int* __restrict__ ibz, int Nz, int Nf, int Nb, double aux) {
+  const size_t n2 = (size_t)Nz * Nz;
+  const size_t n = n2 * Nb;
+  const int r = blockIdx.y;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    cplx f = __ldcs(P.Phi[r] + e);
+    const int i = (int)(e % Nz), j = (int)((e / Nz) % Nz);
+    if (i < Nf && j < Nf) {
+      const int q = (int)(e / n2);
+      const int W = ibz[3 * q + 2];
+      const cplx lam = P.L[r][(size_t)i + (size_t)Nf * (j + (size_t)Nf * (W - 1))];
+      f = cadd(f, cscale(lam, aux));
+    }
+    P.F[r][e] = f;
+  }
+}
+
+// One CTA per (tile of 32 listed elements, target pair x column chunk, q) for
+// one family: C^T[(target, element), (l1,l2)] = X^T[(target, element), (l3,l4,R)] M^T
+// and F_target += C / Nx.  Warps: 4 along rows (16 rows each) x WN along
+// the (l1,l2) columns, TN n8 tiles each; BN = 8 TN WN >= Nl^2 (or a chunk).
 template <int TN, int WN>
-#ifndef PAE_MIN_BLOCKS
-// CTAs per SM requested from ptxas for the 8-warp, 2-tile config: 3 (80
-// registers, a few spilled) runs the 8x8 / Nl=5 loop's crossing step in
-// 2.35 ms against 3.95 ms at 1 (126 registers, 2 CTAs/SM) on a B200
-#define PAE_MIN_BLOCKS 3
-#endif
-__global__ void __launch_bounds__(128 * WN, WN == 2 && TN <= 2 ? PAE_MIN_BLOCKS : 1)
-    k_pae_mma(PaePtrs P, const int* __restrict__ ibz,
-                                                      const int* __restrict__ signs, int Nz, int Nf, int Nl, int NIBZ,
-                                                      int NR, int nchunks, double aux, double inv_nx) {
+__global__ void __launch_bounds__(128 * WN, WN == 2 && TN <= 2 ? 3 : 1)
+    k_pae_mma(PaePtrs P, const int4* __restrict__ elems, const int* __restrict__ counts,
+              const int* __restrict__ ibz, const int* __restrict__ signs, int Nz, int Nf, int Nl, int NIBZ, int NR,
+              int nchunks, int fam, double inv_nx) {
   constexpr int BN = 8 * TN * WN;
   constexpr int NT = 128 * WN;
   extern __shared__ __align__(16) unsigned char smraw[];
   cplx* sA = reinterpret_cast<cplx*>(smraw);      // [2][BK][LDA]
   cplx* sB = sA + 2 * PAE_BK * PAE_LDA;           // [2][BN][LDB]
-  __shared__ int e_w2[2][PAE_E], e_a[2][PAE_E], e_b[2][PAE_E], e_tr[2][PAE_E];
+  __shared__ int e_w2[PAE_E], e_a[PAE_E], e_b[PAE_E], e_tr[PAE_E], e_nu1[PAE_E], e_nu2[PAE_E];
   __shared__ double s_sg[16];
+  __shared__ double fac[2][2];
+  __shared__ int src0;
 
-  const int tiles_x = (Nf + PAE_TX - 1) / PAE_TX;
-  const int nu1_0 = (blockIdx.x % tiles_x) * PAE_TX, nu2_0 = (blockIdx.x / tiles_x) * PAE_TY;
   const int pair = blockIdx.y / nchunks, chunk = blockIdx.y % nchunks;
   // slots ordered with the bosonic frequency outermost, so that the CTAs in
   // flight share the same band of Phi(R) in L2
@@ -149,47 +168,37 @@ __global__ void __launch_bounds__(128 * WN, WN == 2 && TN <= 2 ? PAE_MIN_BLOCKS 
   const int W = ibz[3 * q + 2];
   const int Qi = q / (Nf / 2);
   const int nh = Nf / 2;
+  const int list = pae_list(pair, fam, W, nh);
+  const int cnt = counts[list];
+  const int e0 = blockIdx.x * PAE_E;
+  if (e0 >= cnt) return;
   const int nl2 = Nl * Nl, nl4 = nl2 * nl2;
-  const int KF = nl2 * NR;  // k per family
-  const int K = 2 * KF;
+  const int K = nl2 * NR;
   const size_t n2 = (size_t)Nz * Nz;
   const int tid = threadIdx.x;
 
-  // per-element family maps, and whether the tile is reached by each family
-  int reach0 = 0, reach1 = 0;
-  if (tid < 2 * PAE_E) {
-    const int fam = tid / PAE_E, e = tid % PAE_E;
-    const int nu1 = nu1_0 + e % PAE_TX + 1, nu2 = nu2_0 + e / PAE_TX + 1;
-    int w2 = 0, a = 1, b = 1, tr = 0;
-    bool ok = nu1 <= Nf && nu2 <= Nf && pae_family(pair, fam, nu1, nu2, W, Nf, &w2, &a, &b, &tr);
-    e_w2[fam][e] = ok ? w2 : 0;
-    e_a[fam][e] = a;
-    e_b[fam][e] = b;
-    e_tr[fam][e] = tr;
-    if (ok) {
-      if (fam == 0) reach0 = 1;
-      else reach1 = 1;
-    }
+  if (tid < PAE_E) {
+    int4 rec = make_int4(0, 0, 1, 1);
+    if (e0 + tid < cnt) rec = elems[(size_t)list * Nf * Nf + e0 + tid];
+    e_nu1[tid] = rec.x & 255;
+    e_nu2[tid] = rec.x >> 8;
+    e_w2[tid] = rec.y;
+    e_a[tid] = rec.z;
+    e_b[tid] = rec.w & 65535;
+    e_tr[tid] = rec.w >> 16;
   }
-  const int anyD = __syncthreads_or(reach0);
-  const int anyA = __syncthreads_or(reach1);
   if (tid < Nl) s_sg[tid] = (double)signs[tid];
-  // dispatch factors fac[fam][source][target] (SRC/parquet_EQOuter.f90:84-113)
-  // and the first source channel of each family
-  __shared__ double fac[2][2][2];
-  __shared__ int src0[2];
   if (tid == 0) {
+    // dispatch factors fac[source][target] of this family (SRC/parquet_EQOuter.f90:84-113)
     // pair 0: D = phbar_to_ph from (d, m), A = pp_to_ph from (s, t)
     // pair 1: D = phbar_to_pp from (d, m), A = ph_to_pp from (d, m)
     const double f0[2][2][2] = {{{-0.5, -0.5}, {-1.5, 0.5}}, {{0.5, -0.5}, {1.5, 0.5}}};
     const double f1[2][2][2] = {{{0.5, -0.5}, {-1.5, -0.5}}, {{0.5, 0.5}, {-1.5, 0.5}}};
-    for (int x = 0; x < 2; x++)
-      for (int y = 0; y < 2; y++)
-        for (int z = 0; z < 2; z++) fac[x][y][z] = pair == 0 ? f0[x][y][z] : f1[x][y][z];
-    src0[0] = 0;
-    src0[1] = pair == 0 ? 2 : 0;
+    for (int y = 0; y < 2; y++)
+      for (int z = 0; z < 2; z++) fac[y][z] = pair == 0 ? f0[fam][y][z] : f1[fam][y][z];
+    src0 = (fam == 1 && pair == 0) ? 2 : 0;
   }
-  const cplx* Mf[2] = {P.M[pair == 0 ? 0 : 3], P.M[pair == 0 ? 1 : 2]};
+  const cplx* Mf = P.M[pair == 0 ? (fam == 0 ? 0 : 1) : (fam == 0 ? 3 : 2)];
   __syncthreads();
 
   // gather of one K step into registers: thread -> (element, kk) pairs
@@ -204,22 +213,20 @@ __global__ void __launch_bounds__(128 * WN, WN == 2 && TN <= 2 ? PAE_MIN_BLOCKS 
       const int e = p % PAE_E, kk = p / PAE_E;
       const int k = kt * PAE_BK + kk;
       if (k >= K) continue;
-      const int fam = k / KF, kf = k % KF;
-      const int w2 = e_w2[fam][e];
+      const int w2 = e_w2[e];
       if (w2 == 0) continue;
-      const int l34 = kf % nl2, R = kf / nl2;
+      const int l34 = k % nl2, R = k / nl2;
       const int l3 = l34 % Nl, l4 = l34 / Nl;
-      const size_t xi = (size_t)(l3 * Nf + e_a[fam][e] - 1) + (size_t)Nz * (l4 * Nf + e_b[fam][e] - 1) +
+      const size_t xi = (size_t)(l3 * Nf + e_a[e] - 1) + (size_t)Nz * (l4 * Nf + e_b[e] - 1) +
                         n2 * ((size_t)(w2 - 1) + (size_t)nh * R);
-      const int s0 = src0[fam];
-      cplx x0 = __ldg(P.PhiR[s0] + xi), x1 = __ldg(P.PhiR[s0 + 1] + xi);
-      if (e_tr[fam][e]) {
+      cplx x0 = __ldg(P.PhiR[src0] + xi), x1 = __ldg(P.PhiR[src0 + 1] + xi);
+      if (e_tr[e]) {
         const double sg = s_sg[l3] * s_sg[l4];
         x0 = cmk(sg * x0.x, -sg * x0.y);
         x1 = cmk(sg * x1.x, -sg * x1.y);
       }
-      ra[i] = cmk(fac[fam][0][0] * x0.x + fac[fam][1][0] * x1.x, fac[fam][0][0] * x0.y + fac[fam][1][0] * x1.y);
-      rb[i] = cmk(fac[fam][0][1] * x0.x + fac[fam][1][1] * x1.x, fac[fam][0][1] * x0.y + fac[fam][1][1] * x1.y);
+      ra[i] = cmk(fac[0][0] * x0.x + fac[1][0] * x1.x, fac[0][0] * x0.y + fac[1][0] * x1.y);
+      rb[i] = cmk(fac[0][1] * x0.x + fac[1][1] * x1.x, fac[0][1] * x0.y + fac[1][1] * x1.y);
     }
   };
   auto store_a = [&](int stage) {
@@ -240,11 +247,10 @@ __global__ void __launch_bounds__(128 * WN, WN == 2 && TN <= 2 ? PAE_MIN_BLOCKS 
       const int k = kt * PAE_BK + kk;
       const int col = chunk * BN + n;
       const bool ok = k < K && col < nl2;
-      const cplx* src = Mf[0];
+      const cplx* src = Mf;
       if (ok) {
-        const int fam = k / KF, kf = k % KF;
-        const int l34 = kf % nl2, R = kf / nl2;
-        src = Mf[fam] + col + (size_t)nl2 * l34 + (size_t)nl4 * (Qi + (size_t)NIBZ * R);
+        const int l34 = k % nl2, R = k / nl2;
+        src = Mf + col + (size_t)nl2 * l34 + (size_t)nl4 * (Qi + (size_t)NIBZ * R);
       }
       cp_async16p(dB + n * PAE_LDB + kk, src, ok);
     }
@@ -260,17 +266,12 @@ __global__ void __launch_bounds__(128 * WN, WN == 2 && TN <= 2 ? PAE_MIN_BLOCKS 
 #pragma unroll
     for (int x = 0; x < 4; x++) cre[j][x] = cim[j][x] = 0.0;
 
-  // K steps: skip the half of K that belongs to a family reaching no element
-  // of this tile (its X block is zero)
-  const int kt_lo = anyD ? 0 : KF / PAE_BK;
-  const int kt_hi = anyA ? (K + PAE_BK - 1) / PAE_BK : (KF + PAE_BK - 1) / PAE_BK;
-  if (kt_lo < kt_hi) {
-    gather(kt_lo);
-    load_b(0, kt_lo);
-    store_a(0);
-  }
-  for (int kt = kt_lo; kt < kt_hi; kt++) {
-    const int cur = (kt - kt_lo) & 1;
+  const int kt_hi = (K + PAE_BK - 1) / PAE_BK;
+  gather(0);
+  load_b(0, 0);
+  store_a(0);
+  for (int kt = 0; kt < kt_hi; kt++) {
+    const int cur = kt & 1;
     asm volatile("cp.async.wait_group 0;\n" ::);
     __syncthreads();
     if (kt + 1 < kt_hi) {
@@ -305,9 +306,8 @@ __global__ void __launch_bounds__(128 * WN, WN == 2 && TN <= 2 ? PAE_MIN_BLOCKS 
     if (kt + 1 < kt_hi) store_a(cur ^ 1);
   }
 
-  // epilogue: F = Phi + Lambda*Nc on the (l=1, l=1) block + C/Nx.  Phi and F
-  // are touched once: streaming loads/stores keep them from evicting Phi(R)
-  // and M from L2.
+  // epilogue: F_target += C / Nx on the listed elements (each element is in
+  // a family's list once, so a pass writes it at most once)
 #pragma unroll
   for (int j = 0; j < TN; j++)
 #pragma unroll
@@ -315,22 +315,18 @@ __global__ void __launch_bounds__(128 * WN, WN == 2 && TN <= 2 ? PAE_MIN_BLOCKS 
       const int row = wr * 16 + gid + (x >= 2 ? 8 : 0);
       const int col = chunk * BN + (wc * TN + j) * 8 + 2 * tig + (x & 1);
       const int tgt = row / PAE_E, e = row % PAE_E;
-      const int nu1 = nu1_0 + e % PAE_TX + 1, nu2 = nu2_0 + e / PAE_TX + 1;
-      if (col >= nl2 || nu1 > Nf || nu2 > Nf) continue;
+      if (col >= nl2 || e0 + e >= cnt) continue;
+      const int nu1 = e_nu1[e], nu2 = e_nu2[e];
       const int l1 = col % Nl, l2 = col / Nl;
       const int r = (pair == 0 ? 0 : 2) + tgt;
       const size_t idx = (size_t)(l1 * Nf + nu1 - 1) + (size_t)Nz * (l2 * Nf + nu2 - 1) + n2 * q;
-      cplx f = __ldcs(P.Phi[r] + idx);
-      if (l1 == 0 && l2 == 0) {
-        const cplx lam = P.L[r][(size_t)(nu1 - 1) + (size_t)Nf * ((nu2 - 1) + (size_t)Nf * (W - 1))];
-        f = cadd(f, cscale(lam, aux));
-      }
-      __stcs(P.F[r] + idx, cmk(f.x + inv_nx * cre[j][x], f.y + inv_nx * cim[j][x]));
+      const cplx f = P.F[r][idx];
+      P.F[r][idx] = cmk(f.x + inv_nx * cre[j][x], f.y + inv_nx * cim[j][x]);
     }
 }
 
 template <int TN, int WN>
-static int run_pae(tups_ctx* ctx, const PaePtrs& P, int nchunks) {
+static int run_pae(tups_ctx* ctx, const PaePtrs& P, int nchunks, int fam, int max_tiles) {
   const auto& d = ctx->d;
   constexpr int BN = 8 * TN * WN;
   const size_t sm = (size_t)(2 * PAE_BK * PAE_LDA + 2 * BN * PAE_LDB) * sizeof(cplx);
@@ -339,16 +335,61 @@ static int run_pae(tups_ctx* ctx, const PaePtrs& P, int nchunks) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return cuda_check(ctx, e, "k_pae_mma smem attribute");
   }
-  const int tiles = ((d.Nf + PAE_TX - 1) / PAE_TX) * ((d.Nf + PAE_TY - 1) / PAE_TY);
-  dim3 grid(tiles, 2 * nchunks, d.Nb);
-  kern<<<grid, 128 * WN, sm, ctx->stream>>>(P, ctx->t.ibz, ctx->t.signs, d.Nz, d.Nf, d.Nl, d.NIBZ, d.NR, nchunks,
-                                            std::fabs(1.0 / ctx->FF[0] * 1.0 / ctx->FF[0]), 1.0 / d.Nx);
+  if (max_tiles == 0) return TUPS_OK;
+  dim3 grid(max_tiles, 2 * nchunks, d.Nb);
+  kern<<<grid, 128 * WN, sm, ctx->stream>>>(P, ctx->t.pae_elems, ctx->t.pae_counts, ctx->t.ibz, ctx->t.signs, d.Nz,
+                                            d.Nf, d.Nl, d.NIBZ, d.NR, nchunks, fam, 1.0 / d.Nx);
   return after_launch(ctx, "k_pae_mma");
+}
+
+// Element lists of the two families per target pair and bosonic index W,
+// built on the host from the frequency maps (pae_family) at the first call.
+static int build_pae_lists(tups_ctx* ctx) {
+  const auto& d = ctx->d;
+  const int Nf = d.Nf, nh = Nf / 2;
+  std::vector<int4> el((size_t)4 * nh * Nf * Nf, make_int4(0, 0, 1, 1));
+  std::vector<int> cnt((size_t)4 * nh, 0);
+  for (int pair = 0; pair < 2; pair++)
+    for (int fam = 0; fam < 2; fam++)
+      for (int W = 1; W <= nh; W++) {
+        const int L = pae_list(pair, fam, W, nh);
+        int c = 0;
+        for (int nu2 = 1; nu2 <= Nf; nu2++)
+          for (int nu1 = 1; nu1 <= Nf; nu1++) {
+            int w2, a, b, tr;
+            if (!pae_family(pair, fam, nu1, nu2, W, Nf, &w2, &a, &b, &tr)) continue;
+            el[(size_t)L * Nf * Nf + c++] = make_int4(nu1 + 256 * nu2, w2, a, b + 65536 * tr);
+          }
+        cnt[L] = c;
+        ctx->pae_max_tiles[fam] = std::max(ctx->pae_max_tiles[fam], (c + PAE_E - 1) / PAE_E);
+      }
+  void* pe = nullptr;
+  void* pc = nullptr;
+  int rc = cuda_check(ctx, cudaMalloc(&pe, el.size() * sizeof(int4)), "PAE element lists");
+  if (rc) return rc;
+  ctx->allocations.push_back(pe);
+  rc = cuda_check(ctx, cudaMalloc(&pc, cnt.size() * sizeof(int)), "PAE element counts");
+  if (rc) return rc;
+  ctx->allocations.push_back(pc);
+  ctx->t.pae_elems = (int4*)pe;
+  ctx->t.pae_counts = (int*)pc;
+  rc = cuda_check(ctx, cudaMemcpyAsync(pe, el.data(), el.size() * sizeof(int4), cudaMemcpyHostToDevice, ctx->stream),
+                  "PAE lists H2D");
+  if (rc) return rc;
+  rc = cuda_check(ctx, cudaMemcpyAsync(pc, cnt.data(), cnt.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->stream),
+                  "PAE counts H2D");
+  if (rc) return rc;
+  return cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "PAE lists");
 }
 
 int launch_pae(tups_ctx* ctx) {
   const auto& d = ctx->d;
   if (d.Nl > 13) return set_error(ctx, TUPS_ERR_BADDIM, "Nl > 13 not supported by the crossing kernel");
+  if (d.Nf > 255) return set_error(ctx, TUPS_ERR_BADDIM, "Nf > 255 not supported by the crossing kernel");
+  if (!ctx->t.pae_elems) {
+    int rc = build_pae_lists(ctx);
+    if (rc) return rc;
+  }
   PaePtrs P;
   for (int r = 0; r < 4; r++) {
     P.Phi[r] = ctx->s.G[r];
@@ -357,10 +398,21 @@ int launch_pae(tups_ctx* ctx) {
     P.L[r] = ctx->t.L[r];
     P.F[r] = ctx->s.F[r];
   }
+  // F = Phi + Lambda Nc, then the diagonal family, then the anti-diagonal one
+  const size_t n = (size_t)d.Nz * d.Nz * d.Nb;
+  dim3 bgrid((unsigned)std::min<size_t>(cdiv(n, 256), 148 * 8), 4);
+  k_pae_base<<<bgrid, 256, 0, ctx->stream>>>(P, ctx->t.ibz, d.Nz, d.Nf, d.Nb, std::fabs(1.0 / ctx->FF[0] * 1.0 / ctx->FF[0]));
+  int rc = after_launch(ctx, "k_pae_base");
+  if (rc) return rc;
   const int nl2 = d.Nl * d.Nl;
-  if (nl2 <= 8) return run_pae<1, 1>(ctx, P, 1);
-  if (nl2 <= 32) return run_pae<2, 2>(ctx, P, 1);
-  return run_pae<6, 2>(ctx, P, (nl2 + 95) / 96);
+  for (int fam = 0; fam < 2; fam++) {
+    const int mt = ctx->pae_max_tiles[fam];
+    if (nl2 <= 8) rc = run_pae<1, 1>(ctx, P, 1, fam, mt);
+    else if (nl2 <= 32) rc = run_pae<2, 2>(ctx, P, 1, fam, mt);
+    else rc = run_pae<6, 2>(ctx, P, (nl2 + 95) / 96, fam, mt);
+    if (rc) return rc;
+  }
+  return TUPS_OK;
 }
 
 }  // namespace tups

@@ -33,6 +33,8 @@ struct DeviceTables {
   cplx* tw_tau = nullptr;     // (Nf tau, Nf nu) e^{-i nu_n tau_i}
   cplx* tw_x = nullptr;       // (Nx*Ng) e^{-2 pi i m / n1}
   cplx* tw_y = nullptr;       // (Ny*Ng)
+  int4* pae_elems = nullptr;  // crossing: elements per (pair, family, W), see pae.cu
+  int* pae_counts = nullptr;
 };
 
 struct DeviceState {
@@ -112,6 +114,7 @@ struct tups_ctx {
   // host copies of small state
   double F_max_prev[4] = {0, 0, 0, 0};
   bool have_exp = false, have_M = false, have_phir = false, have_green = false;
+  int pae_max_tiles[2] = {0, 0};  // CTAs along the element lists of each family
   tups::DeviceTables t;
   tups::DeviceState s;
   tups::ReadoutBufs rd;
