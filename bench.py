@@ -224,15 +224,11 @@ def run_reference(args, wl_name: str, wl: dict):
 
 def run_tups(args, wl_name: str, wl: dict):
     import torch
+    from tups_b200 import replicas
     ws, rank, local = dist_env()
     device = local
     torch.cuda.set_device(device)
-    pg = None
-    if ws > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
-        pg = dist
+    ranks = replicas.init("nccl")
     from tups_b200 import Params, Solver, load
     load()
     peak64 = fp64_peak_tflops(device)
@@ -247,8 +243,7 @@ def run_tups(args, wl_name: str, wl: dict):
     # ---- timed region: K iterations, device-resident state ----
     sol.set_timing(True)
     l0 = sol.kernel_launches
-    if pg:
-        pg.barrier()
+    replicas.barrier(ranks)
     torch.cuda.synchronize(device)
     sol.synchronize()
     clocks = ClockSampler(device)
@@ -270,8 +265,7 @@ def run_tups(args, wl_name: str, wl: dict):
     h_in = torch.empty(2 * nt, dtype=torch.float64, pin_memory=True).numpy().view(np.complex128)
     h_out = torch.empty(2 * nt, dtype=torch.float64, pin_memory=True).numpy().view(np.complex128)
     h_in[:] = sol.Sigma
-    if pg:
-        pg.barrier()
+    replicas.barrier(ranks)
     sol.synchronize()
     sol.record_event(2)
     for k in range(K):
@@ -282,12 +276,9 @@ def run_tups(args, wl_name: str, wl: dict):
     sol.record_event(3)
     ms_e2e = sol.event_elapsed_ms(2, 3)
     # ---- max over ranks ----
-    if pg:
-        t = torch.tensor([ms, ms_e2e], dtype=torch.float64, device=f"cuda:{device}")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms, ms_e2e = float(t[0]), float(t[1])
-    value = ms * 1e-3 / (K * ws)
-    e2e_value = ms_e2e * 1e-3 / (K * ws)
+    ms, ms_e2e = replicas.max_over_ranks(ranks, [ms, ms_e2e])
+    value = replicas.seconds_per_iteration(ms, K, ws)
+    e2e_value = replicas.seconds_per_iteration(ms_e2e, K, ws)
     d = sol.dims
     # ---- roofline of the kernels ----
     tab = sol.tables()
@@ -324,7 +315,7 @@ def run_tups(args, wl_name: str, wl: dict):
     bse_tflops = kern.get("k_bse_gemm", {}).get("achieved")
     split = None
     conv = None
-    if not args.no_split:
+    if not args.no_split and ws == 1:
         split = split_iterations(params, device, K, W, Nz, Nb, peak64)
         if Nz <= 256 and not args.no_convergence:
             conv = to_convergence(params, device)
@@ -362,9 +353,7 @@ def run_tups(args, wl_name: str, wl: dict):
         }
         print(json.dumps(line), flush=True)
     sol.close()
-    if pg:
-        pg.barrier()
-        pg.destroy_process_group()
+    replicas.finish(ranks)
 
 
 SPLIT_SLICES = (3, 5, 7, 8)
