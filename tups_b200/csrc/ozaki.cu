@@ -47,6 +47,50 @@ __device__ __forceinline__ const cplx* oz_part(const OzOperand& o, int part, int
   return part == 1 ? o.p1 + (size_t)o.s1 * inst : o.p2 + (size_t)o.s2 * inst;
 }
 
+// Per-instance view of an operand
+struct OzLine {
+  const cplx* p1;
+  const cplx* p2;
+  int ld1, ld2, K1;
+  const cplx* G;
+  const cplx* F;
+  const cplx* chi;
+  int Nz, Nf, Nl, mode;
+};
+
+__device__ __forceinline__ OzLine oz_view(const OzOperand& o, int inst) {
+  OzLine v;
+  v.mode = o.mode;
+  v.ld1 = o.ld1;
+  v.ld2 = o.ld2;
+  v.K1 = o.K1;
+  v.Nz = o.Nz;
+  v.Nf = o.Nf;
+  v.Nl = o.Nl;
+  v.p1 = v.p2 = v.G = v.F = v.chi = nullptr;
+  if (o.mode == 0) {
+    v.p1 = oz_part(o, 1, inst);
+    v.p2 = o.K2 ? oz_part(o, 2, inst) : nullptr;
+  } else {
+    const int q = o.q_begin + inst / 4, r = inst % 4;
+    const size_t off = (size_t)o.Nz * o.Nz * q;
+    v.G = o.G[r] + off;
+    v.F = o.F[r] + off;
+    v.chi = (r < 2 ? o.chi_ph : o.chi_pp) + (size_t)o.Nl * o.Nl * o.Nf * q;
+  }
+  return v;
+}
+
+// element (m, k) of a row operand (parts)
+__device__ __forceinline__ cplx oz_a(const OzLine& v, int m, int k) {
+  return k < v.K1 ? v.p1[m + (size_t)v.ld1 * k] : v.p2[m + (size_t)v.ld2 * (k - v.K1)];
+}
+
+// element (k, j) of a column operand (parts)
+__device__ __forceinline__ cplx oz_b(const OzLine& v, int k, int j) {
+  return k < v.K1 ? v.p1[k + (size_t)v.ld1 * j] : v.p2[(k - v.K1) + (size_t)v.ld2 * j];
+}
+
 // s int8 slices of v * 2^-e into out[i * slice_stride], |v 2^-e| < 1
 __device__ __forceinline__ void oz_cut(double v, int e, int s, int8_t* out, size_t slice_stride) {
   double r = ldexp(v, -e);
@@ -70,8 +114,7 @@ __global__ void __launch_bounds__(256) k_oz_split_rows(OzOperand A, int M, int s
   const int inst = blockIdx.y;
   const int m0 = blockIdx.x * 32;
   const int Kc = A.K1 + A.K2;
-  const cplx* X1 = oz_part(A, 1, inst);
-  const cplx* X2 = A.K2 ? oz_part(A, 2, inst) : nullptr;
+  const OzLine V = oz_view(A, inst);
   __shared__ double smax[8][33];
   __shared__ int sexp[32];
   __shared__ cplx tile[32][33];
@@ -81,7 +124,7 @@ __global__ void __launch_bounds__(256) k_oz_split_rows(OzOperand A, int M, int s
     double mx = 0.0;
     if (m < M)
       for (int k = w; k < Kc; k += 8) {
-        const cplx v = k < A.K1 ? X1[m + (size_t)A.ld1 * k] : X2[m + (size_t)A.ld2 * (k - A.K1)];
+        const cplx v = oz_a(V, m, k);
         mx = fmax(mx, fmax(fabs(v.x), fabs(v.y)));
       }
     smax[w][lane] = mx;
@@ -106,7 +149,7 @@ __global__ void __launch_bounds__(256) k_oz_split_rows(OzOperand A, int M, int s
       const int r = e & 31, c = e >> 5;
       const int m = m0 + r, k = k0 + c;
       cplx v = cmk(0.0, 0.0);
-      if (m < M && k < Kc) v = k < A.K1 ? X1[m + (size_t)A.ld1 * k] : X2[m + (size_t)A.ld2 * (k - A.K1)];
+      if (m < M && k < Kc) v = oz_a(V, m, k);
       tile[c][r] = v;
     }
     __syncthreads();
@@ -144,22 +187,44 @@ __global__ void __launch_bounds__(256) k_oz_split_rows(OzOperand A, int M, int s
   }
 }
 
-// Columns of B': one warp per complex column j of B (K1 + K2 long); writes
-// rows 2j and 2j+1 of every slice.  out: [inst][s][2N][Kpad].
-__global__ void __launch_bounds__(256) k_oz_split_cols(OzOperand B, int N, int s, int Kpad, int8_t* __restrict__ out,
+// Columns of B': one warp per complex column j of B (K1 + K2 long), staged
+// in shared memory (mode 2 also stages the Gamma column and forms chi Gamma
+// from it); writes rows 2j and 2j+1 of every slice.  out: [inst][s][2N][Kpad].
+__global__ void __launch_bounds__(128) k_oz_split_cols(OzOperand B, int N, int s, int Kpad, int8_t* __restrict__ out,
                                                        double* __restrict__ cscale) {
+  extern __shared__ __align__(16) unsigned char oz_cols_sm[];
   const int inst = blockIdx.y;
-  const int j = blockIdx.x * 8 + (threadIdx.x >> 5);
+  const int wib = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+  const int j = blockIdx.x * wpb + wib;
   const int lane = threadIdx.x & 31;
   if (j >= N) return;
   const int Kc = B.K1 + B.K2;
-  const cplx* Y1 = oz_part(B, 1, inst) + (size_t)B.ld1 * j;
-  const cplx* Y2 = B.K2 ? oz_part(B, 2, inst) + (size_t)B.ld2 * j : nullptr;
-  double mx = 0.0;
-  for (int k = lane; k < Kc; k += 32) {
-    const cplx v = k < B.K1 ? Y1[k] : Y2[k - B.K1];
-    mx = fmax(mx, fmax(fabs(v.x), fabs(v.y)));
+  const int gz = B.mode == 2 ? B.Nz : 0;
+  cplx* col = reinterpret_cast<cplx*>(oz_cols_sm) + (size_t)wib * (Kc + gz);
+  cplx* gcol = col + Kc;
+  const OzLine V = oz_view(B, inst);
+  if (B.mode == 2) {
+    for (int k = lane; k < B.Nz; k += 32) gcol[k] = V.G[k + (size_t)B.Nz * j];
+    __syncwarp();
+    for (int k = lane; k < Kc; k += 32) {
+      cplx v;
+      if (k < B.Nz) {
+        v = V.F[k + (size_t)B.Nz * j];
+      } else {
+        // (chi Gamma)[(l1, nu), j], summed in the order of k_bse_prep
+        const int kk = k - B.Nz, l1 = kk / B.Nf, nu = kk % B.Nf;
+        v = cmk(0.0, 0.0);
+        for (int l2 = 0; l2 < B.Nl; l2++)
+          v = cfma(__ldg(V.chi + l1 + B.Nl * (l2 + (size_t)B.Nl * nu)), gcol[l2 * B.Nf + nu], v);
+      }
+      col[k] = v;
+    }
+  } else {
+    for (int k = lane; k < Kc; k += 32) col[k] = oz_b(V, k, j);
   }
+  __syncwarp();
+  double mx = 0.0;
+  for (int k = lane; k < Kc; k += 32) mx = fmax(mx, fmax(fabs(col[k].x), fabs(col[k].y)));
   mx = warp_max(mx);
   const int e = oz_exponent(mx);
   if (lane == 0) cscale[(size_t)inst * N + j] = ldexp(1.0, e);
@@ -167,26 +232,25 @@ __global__ void __launch_bounds__(256) k_oz_split_cols(OzOperand B, int N, int s
   int8_t* r0 = out + (size_t)inst * s * slice_stride + (size_t)(2 * j) * Kpad;
   int8_t* r1 = r0 + Kpad;
   for (int k = lane * 4; k < Kc; k += 128) {
-    int8_t re[4][8], im[4][8], nim[4][8];
+    int8_t re[4][8], im[4][8];
     for (int c = 0; c < 4; c++) {
-      const int kk = k + c;
-      const cplx v = kk < Kc ? (kk < B.K1 ? Y1[kk] : Y2[kk - B.K1]) : cmk(0.0, 0.0);
+      const cplx v = k + c < Kc ? col[k + c] : cmk(0.0, 0.0);
       oz_cut(v.x, e, s, &re[c][0], 1);
       oz_cut(v.y, e, s, &im[c][0], 1);
-      oz_cut(-v.y, e, s, &nim[c][0], 1);
     }
+    // the slices of -Im are the negated slices of Im (truncation is odd)
     for (int i = 0; i < s; i++) {
       int8_t* d0 = r0 + (size_t)i * slice_stride;
       int8_t* d1 = r1 + (size_t)i * slice_stride;
       if ((Kc & 3) == 0 && k + 3 < Kc) {
         *reinterpret_cast<char4*>(d0 + k) = make_char4(re[0][i], re[1][i], re[2][i], re[3][i]);
-        *reinterpret_cast<char4*>(d0 + Kc + k) = make_char4(nim[0][i], nim[1][i], nim[2][i], nim[3][i]);
+        *reinterpret_cast<char4*>(d0 + Kc + k) = make_char4(-im[0][i], -im[1][i], -im[2][i], -im[3][i]);
         *reinterpret_cast<char4*>(d1 + k) = make_char4(im[0][i], im[1][i], im[2][i], im[3][i]);
         *reinterpret_cast<char4*>(d1 + Kc + k) = make_char4(re[0][i], re[1][i], re[2][i], re[3][i]);
       } else {
         for (int c = 0; c < 4 && k + c < Kc; c++) {
           d0[k + c] = re[c][i];
-          d0[Kc + k + c] = nim[c][i];
+          d0[Kc + k + c] = (int8_t)(-im[c][i]);
           d1[k + c] = im[c][i];
           d1[Kc + k + c] = re[c][i];
         }
@@ -639,8 +703,16 @@ int oz_run(OzRun& R, cudaStream_t stream, long long* launches) {
     dim3 g((M + 31) / 32, batch);
     k_oz_split_rows<<<g, 256, 0, stream>>>(R.A, M, s, Kpad, R.a_slices, R.rscale);
     if (launches) (*launches)++;
-    dim3 gc((N + 7) / 8, batch);
-    k_oz_split_cols<<<gc, 256, 0, stream>>>(R.B, N, s, Kpad, R.b_slices, R.cscale);
+    // column splitter: up to 4 warps per CTA, one staged column each
+    const size_t per_warp = (size_t)(K + (R.B.mode == 2 ? R.B.Nz : 0)) * sizeof(cplx);
+    const int wpb = (int)std::max<size_t>(1, std::min<size_t>(4, (200 * 1024) / per_warp));
+    if (per_warp > 200 * 1024) return TUPS_ERR_BADDIM;
+    const size_t csm = per_warp * wpb;
+    if (csm > 48 * 1024 &&
+        cudaFuncSetAttribute(k_oz_split_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm) != cudaSuccess)
+      return TUPS_ERR_CUDA;
+    dim3 gc((N + wpb - 1) / wpb, batch);
+    k_oz_split_cols<<<gc, 32 * wpb, csm, stream>>>(R.B, N, s, Kpad, R.b_slices, R.cscale);
     if (launches) (*launches)++;
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return TUPS_ERR_CUDA;
