@@ -315,8 +315,10 @@ def run_tups(args, wl_name: str, wl: dict):
     bse_tflops = kern.get("k_bse_gemm", {}).get("achieved")
     split = None
     conv = None
+    graph = None
     if not args.no_split and ws == 1:
         split = split_iterations(params, device, K, W, Nz, Nb, peak64)
+        graph = graph_iterations(params, device, K, W)
         if Nz <= 256 and not args.no_convergence:
             conv = to_convergence(params, device)
     cpu = None
@@ -339,6 +341,7 @@ def run_tups(args, wl_name: str, wl: dict):
                        "parallelism": "replicas" if ws > 1 else "single GPU"},
             "bse_tflops": bse_tflops,
             "split_precision": split,
+            "cuda_graph": graph,
             "to_convergence": conv,
             "roofline": roof,
             "kernels": kern,
@@ -388,6 +391,26 @@ def split_iterations(params, device: int, K: int, W: int, Nz: int, Nb: int, peak
     out["note"] = ("effective TFLOP/s = FP64-equivalent 16 Nz^3 per (q, r) / split GEMM time; int8_tops = "
                    "s(s+1)/2 slice products x 2 M (2N) (2K) / time")
     return out
+
+
+def graph_iterations(params, device: int, K: int, W: int) -> dict:
+    """The same K iterations replayed from a captured CUDA graph (one host
+    synchronisation per iteration)."""
+    from tups_b200 import Solver
+    sol = Solver(params, device=device)
+    sol.set_graph(True)
+    for ite in range(W):
+        sol.iteration(ite)
+    sol.synchronize()
+    l0 = sol.kernel_launches
+    sol.record_event(0)
+    for k in range(K):
+        sol.iteration(W + k)
+    sol.record_event(1)
+    ms = sol.event_elapsed_ms(0, 1) / K
+    launches = (sol.kernel_launches - l0) / K
+    sol.close()
+    return {"ms_per_iter": ms, "kernels_per_iter": launches}
 
 
 def to_convergence(params, device: int, max_iter: int = 3000) -> dict:

@@ -161,6 +161,11 @@ int tups_output_block(tups_ctx* ctx);
 /* one pass of execute_loop (SRC/loop.f90:51-244) without the readout: on
  * output iterations only the readout's effect on mu is applied */
 int tups_iteration(tups_ctx* ctx, int ite, tups_conv_info* info);
+/* enable = 1: tups_iteration (from ite 1 on, phase timing off) replays the
+ * iteration's device work from a CUDA graph captured on first use per
+ * precision choice, with one host synchronisation per iteration.  No
+ * counterpart in the reference. */
+int tups_set_graph(tups_ctx* ctx, int enable);
 /* execute_loop (SRC/loop.f90:29-249) including the readout of every output
  * iteration (SRC/loop.f90:181-213; results via tups_get_chi0/tups_get_sus);
  * *ite_out = iterations done */

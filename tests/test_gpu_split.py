@@ -118,3 +118,42 @@ def test_fixed_slices_loop_reaches_the_fp64_fixed_point(gpu_lib):
         sol.close()
     # 7 slices: GEMM error ~1e-13 relative; the fixed points agree to 1e-10
     assert parity.rel(sols[7], sols[0]) <= 1e-10
+
+
+def test_graph_iterations_equal_plain_ones(gpu_lib):
+    from tups_b200 import Params, Solver
+    p = Params(beta=3.0, U=2.0, nParticle=0.9, Nx=4, Nf=8, neighbours=2, tprime=-0.1, f_damping=0.5,
+               ite_max=100)
+    out = {}
+    for graph in (False, True):
+        sol = Solver(p)
+        sol.set_graph(graph)
+        infos = [sol.iteration(i) for i in range(7)]   # ite 5 applies the output block
+        out[graph] = (sol.Sigma, sol.F(0), sol.G(2), sol.mu, [c["dsigma_inf"] for c in infos],
+                      sol.kernel_launches)
+        sol.close()
+    a, b = out[False], out[True]
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]) and np.array_equal(a[2], b[2])
+    assert a[3] == b[3] and a[4] == b[4]
+    assert b[5] == a[5]     # graph replays count their kernels
+
+
+def test_graph_with_ladder_converges(gpu_lib):
+    from tups_b200 import Params, Solver
+    p = Params(beta=3.0, U=2.0, nParticle=0.9, Nx=4, Nf=8, neighbours=2, tprime=-0.1, f_damping=0.5,
+               ite_max=10 ** 6, conv_abs=1e-10)
+    ref = Solver(p)
+    n = 0
+    while not ref.iteration(n)["converged"]:
+        n += 1
+    sig = ref.Sigma
+    ref.close()
+    sol = Solver(p)
+    sol.set_graph(True)
+    sol.set_bse_precision(0, ladder=True)
+    m = 0
+    while not sol.iteration(m)["converged"]:
+        m += 1
+        assert m < 3 * n + 10
+    assert parity.rel(sol.Sigma, sig) <= 1e-10 * 50
+    sol.close()

@@ -103,6 +103,7 @@ _PROTOS = {
                          C.c_double, C.c_void_p],
     "tups_set_timing": [C.c_void_p, C.c_int],
     "tups_set_bse_precision": [C.c_void_p, C.c_int, C.c_int],
+    "tups_set_graph": [C.c_void_p, C.c_int],
     "tups_zgemm_split": [C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
                          C.c_void_p, C.c_size_t, C.c_void_p],
     "tups_mlp_create": [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p)],

@@ -66,11 +66,12 @@ int green_async(tups_ctx* ctx, int cal_chi) {
   return TUPS_OK;
 }
 
-int bse_async(tups_ctx* ctx) {
+int bse_async(tups_ctx* ctx, int slices = -1) {
   if (!ctx->have_green) return tups::set_error(ctx, TUPS_ERR_STATE, "BSE before calc_Gkw_Grt");
   const int Nb = ctx->d.Nb;
-  ctx->cur_slices = tups::current_bse_slices(ctx);
-  const bool tune = ctx->precision_ladder;
+  ctx->cur_slices = slices >= 0 ? slices : tups::current_bse_slices(ctx);
+  // the tuner times whole BSE calls outside graphs; graph mode times the graph
+  const bool tune = ctx->precision_ladder && !ctx->capturing && !ctx->use_graph;
   if (tune) {
     for (int i = 0; i < 2; i++)
       if (!ctx->tune_ev[i]) TRY(tups::cuda_check(ctx, cudaEventCreate(&ctx->tune_ev[i]), "event"));
@@ -195,14 +196,8 @@ extern "C" int tups_calc_SDE(tups_ctx* ctx, int ite) {
   return tups::cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "calc_SDE");
 }
 
-extern "C" int tups_conv(tups_ctx* ctx, tups_conv_info* info) {
-  if (!ctx) return TUPS_ERR_BADARG;
-  TRY(set_dev(ctx));
-  tups::phase_begin(ctx, TUPS_PHASE_CONV);
-  TRY(tups::launch_conv(ctx));
-  tups::phase_end(ctx, TUPS_PHASE_CONV);
-  double sc[tups::S_COUNT];
-  TRY(read_scalars(ctx, sc));
+// conv()'s host decision from the device scalars (SRC/parquet_check.f90:39-150)
+static int conv_finish(tups_ctx* ctx, const double* sc, tups_conv_info* info) {
   tups_conv_info ci;
   std::memset(&ci, 0, sizeof(ci));
   ci.rel_sig_max = sc[tups::S_RELSIG];
@@ -223,15 +218,33 @@ extern "C" int tups_conv(tups_ctx* ctx, tups_conv_info* info) {
   if (ctx->p.conv_abs > 0.0) ok = ci.dsigma_inf < ctx->p.conv_abs;
   ci.converged = ok ? 1 : 0;
   ctx->last_dsigma_rel = sc[tups::S_SIGMAX] > 0.0 ? ci.dsigma_inf / sc[tups::S_SIGMAX] : -1.0;
-  tups::bse_tune_collect(ctx);  // read_scalars synchronised the stream
-  const size_t bytes = (size_t)ctx->d.Nt * sizeof(cplx);
-  TRY(tups::cuda_check(ctx,
-                       cudaMemcpyAsync(ctx->s.SigmaOld, ctx->s.Sigma, bytes, cudaMemcpyDeviceToDevice, ctx->stream),
-                       "SigmaOld = Sigma"));
+  tups::bse_tune_collect(ctx);  // the caller synchronised the stream
   if (info) *info = ci;
   if (sc[tups::S_NANFLAG] > 0.0 || !std::isfinite(ci.rel_sig_max))
     return tups::set_error(ctx, TUPS_ERR_NAN, "NaN or Inf in the self-energy or a vertex");
   return TUPS_OK;
+}
+
+static int copy_sigma_old(tups_ctx* ctx) {
+  const size_t bytes = (size_t)ctx->d.Nt * sizeof(cplx);
+  return tups::cuda_check(
+      ctx, cudaMemcpyAsync(ctx->s.SigmaOld, ctx->s.Sigma, bytes, cudaMemcpyDeviceToDevice, ctx->stream),
+      "SigmaOld = Sigma");
+}
+
+extern "C" int tups_conv(tups_ctx* ctx, tups_conv_info* info) {
+  if (!ctx) return TUPS_ERR_BADARG;
+  TRY(set_dev(ctx));
+  tups::phase_begin(ctx, TUPS_PHASE_CONV);
+  TRY(tups::launch_conv(ctx));
+  tups::phase_end(ctx, TUPS_PHASE_CONV);
+  double sc[tups::S_COUNT];
+  TRY(read_scalars(ctx, sc));
+  tups_conv_info ci;
+  const int rc = conv_finish(ctx, sc, &ci);
+  TRY(copy_sigma_old(ctx));
+  if (info) *info = ci;
+  return rc;
 }
 
 extern "C" int tups_vertex_update(tups_ctx* ctx) {
@@ -332,9 +345,89 @@ extern "C" int tups_get_sus(tups_ctx* ctx, int channel, int bz, double* host) {
 }
 
 static int iteration_impl(tups_ctx* ctx, int ite, tups_conv_info* info, bool with_readout);
+static int iteration_graph(tups_ctx* ctx, int ite, tups_conv_info* info);
 
 extern "C" int tups_iteration(tups_ctx* ctx, int ite, tups_conv_info* info) {
+  if (ctx && ctx->use_graph && ite > 0 && ctx->have_exp && ctx->have_M && !ctx->timing)
+    return iteration_graph(ctx, ite, info);
   return iteration_impl(ctx, ite, info, false);
+}
+
+// The device work of one iteration with no host synchronisation: Green's
+// function, BSE, Phi(R), parquet equation, SDE, the conv kernels,
+// SigmaOld = Sigma and the vertex update.  The output block only moves mu
+// and does not touch the vertices, so it follows the update on the host.
+static int iteration_device(tups_ctx* ctx, int slices, bool do_sde) {
+  TRY(green_async(ctx, 0));
+  TRY(bse_async(ctx, slices));
+  TRY(tups::launch_phir(ctx));
+  TRY(tups::launch_pae(ctx));
+  if (do_sde) TRY(sde_async(ctx));
+  TRY(tups::launch_conv(ctx));
+  TRY(copy_sigma_old(ctx));
+  return tups::launch_vertex_update(ctx);
+}
+
+// One iteration replayed from a CUDA graph captured on first use for each
+// (slices, SDE) choice, then one read of the device scalars.
+static int iteration_graph(tups_ctx* ctx, int ite, tups_conv_info* info) {
+  TRY(set_dev(ctx));
+  const int sl = tups::current_bse_slices(ctx);
+  const bool do_sde = !ctx->p.oneshot || ite == ctx->p.ite_max - 1;
+  const int key = sl * 2 + (do_sde ? 1 : 0);
+  if (!ctx->graph_exec[key]) {
+    const long long l0 = ctx->launches;
+    TRY(tups::cuda_check(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed), "begin capture"));
+    ctx->capturing = true;
+    const int rc = iteration_device(ctx, sl, do_sde);
+    ctx->capturing = false;
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+    if (rc) {
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();
+      return rc;
+    }
+    TRY(tups::cuda_check(ctx, e, "end capture"));
+    e = cudaGraphInstantiate(&ctx->graph_exec[key], g, 0);
+    cudaGraphDestroy(g);
+    TRY(tups::cuda_check(ctx, e, "graph instantiate"));
+    ctx->graph_launches[key] = ctx->launches - l0;
+    ctx->launches = l0;
+  }
+  const bool tune = ctx->precision_ladder;
+  if (tune) {
+    for (int i = 0; i < 2; i++)
+      if (!ctx->tune_ev[i]) TRY(tups::cuda_check(ctx, cudaEventCreate(&ctx->tune_ev[i]), "event"));
+    TRY(tups::cuda_check(ctx, cudaEventRecord(ctx->tune_ev[0], ctx->stream), "event"));
+  }
+  TRY(tups::cuda_check(ctx, cudaGraphLaunch(ctx->graph_exec[key], ctx->stream), "graph launch"));
+  ctx->launches += ctx->graph_launches[key];
+  if (tune) {
+    TRY(tups::cuda_check(ctx, cudaEventRecord(ctx->tune_ev[1], ctx->stream), "event"));
+    ctx->tune_pending = sl;
+  }
+  double sc[tups::S_COUNT];
+  TRY(read_scalars(ctx, sc));
+  const int st = (int)sc[tups::S_STATUS];
+  if (st != 0) {
+    double z = 0.0;
+    cudaMemcpy(ctx->s.scal + tups::S_STATUS, &z, sizeof(double), cudaMemcpyHostToDevice);
+    return tups::set_error(ctx, st, st == TUPS_ERR_MU_NOCONV ? "mu bisection exceeded its step cap"
+                                                             : "device routine reported an error");
+  }
+  tups_conv_info ci;
+  const int rc = conv_finish(ctx, sc, &ci);
+  if (info) *info = ci;
+  if (rc) return rc;
+  if (ite % 5 == 0 || ite == ctx->p.ite_max - 1 || ci.converged) TRY(tups::launch_output_mu(ctx));
+  return TUPS_OK;
+}
+
+extern "C" int tups_set_graph(tups_ctx* ctx, int enable) {
+  if (!ctx) return TUPS_ERR_BADARG;
+  ctx->use_graph = enable != 0;
+  return TUPS_OK;
 }
 
 static int iteration_impl(tups_ctx* ctx, int ite, tups_conv_info* info, bool with_readout) {

@@ -232,28 +232,29 @@ static int run_gemm(tups_ctx* ctx, const BsePtrs& P, int q_begin, int q_count) {
 // s (s + 1) / 2 slice products; FP64 is timed on the first call.
 int current_bse_slices(const tups_ctx* ctx) {
   if (!ctx->precision_ladder) return ctx->bse_slices;
+  const double* tms = ctx->use_graph ? ctx->tune_graph_ms : ctx->tune_ms;
   const double r = ctx->last_dsigma_rel;
   int s_req = 3;
   if (r == 0.0) s_req = 9;
   else if (r > 0.0) s_req = std::max(2, (int)std::ceil((3.1 - std::log10(r)) / 2.0));
   if (s_req > 8) return 0;
-  if (ctx->tune_ms[0] < 0.0) return 0;
-  double est = ctx->tune_ms[s_req];
+  if (tms[0] < 0.0) return 0;
+  double est = tms[s_req];
   if (est < 0.0) {
     int s0 = -1;
     for (int s = 2; s <= 8; s++)
-      if (ctx->tune_ms[s] >= 0.0 && (s0 < 0 || std::abs(s - s_req) < std::abs(s0 - s_req))) s0 = s;
+      if (tms[s] >= 0.0 && (s0 < 0 || std::abs(s - s_req) < std::abs(s0 - s_req))) s0 = s;
     if (s0 < 0) return s_req;  // nothing measured yet: try it
-    est = ctx->tune_ms[s0] * (double)(s_req * (s_req + 1)) / (double)(s0 * (s0 + 1));
+    est = tms[s0] * (double)(s_req * (s_req + 1)) / (double)(s0 * (s0 + 1));
   }
-  return est < ctx->tune_ms[0] ? s_req : 0;
+  return est < tms[0] ? s_req : 0;
 }
 
 void bse_tune_collect(tups_ctx* ctx) {
   if (ctx->tune_pending < 0) return;
   float ms = 0.0f;
   if (cudaEventElapsedTime(&ms, ctx->tune_ev[0], ctx->tune_ev[1]) == cudaSuccess) {
-    double& slot = ctx->tune_ms[ctx->tune_pending];
+    double& slot = (ctx->use_graph ? ctx->tune_graph_ms : ctx->tune_ms)[ctx->tune_pending];
     slot = slot < 0.0 ? ms : 0.5 * (slot + ms);
   } else {
     cudaGetLastError();

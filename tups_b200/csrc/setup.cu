@@ -666,6 +666,11 @@ void destroy_events(tups_ctx* ctx);
 }
 
 static void free_all(tups_ctx* ctx) {
+  for (auto& g : ctx->graph_exec)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
   tups::destroy_events(ctx);
   for (void* p : ctx->allocations) cudaFree(p);
   ctx->allocations.clear();

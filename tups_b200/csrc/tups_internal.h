@@ -138,6 +138,13 @@ struct tups_ctx {
   int tune_pending = -1;       // choice whose timing events are in flight
   cudaEvent_t tune_ev[2] = {nullptr, nullptr};
   double tune_ms[9] = {-1, -1, -1, -1, -1, -1, -1, -1, -1};  // [0] FP64, [s] s slices
+  // CUDA-graph iterations: one executable graph per (slices, SDE) choice;
+  // in graph mode the tuner compares whole-iteration times (tune_graph_ms)
+  bool use_graph = false;
+  bool capturing = false;
+  cudaGraphExec_t graph_exec[18] = {};
+  long long graph_launches[18] = {};
+  double tune_graph_ms[9] = {-1, -1, -1, -1, -1, -1, -1, -1, -1};
   double ck_scal[16] = {};
   double ck_fmax[4] = {};
   bool ck_valid = false;

@@ -251,6 +251,10 @@ class Solver:
     def synchronize(self) -> None:
         self._call("tups_synchronize")
 
+    def set_graph(self, enable: bool = True) -> None:
+        """Replay iterations (from ite 1 on) from captured CUDA graphs."""
+        self._call("tups_set_graph", int(bool(enable)))
+
     # -- split-precision BSE --
     def set_bse_precision(self, slices: int = 0, ladder: bool = False) -> None:
         """slices = 0: FP64 tensor cores; 2..8: int8 slices per operand;
