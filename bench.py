@@ -7,6 +7,9 @@ U=2, beta=5, n=1, linear mixing 0.5, complex128 storage.  A step is one
 parquet iteration (Green's function + mu bisection, BSE, Phi(R), parquet
 equation, Schwinger-Dyson, convergence check, vertex update).  The state
 (~0.9 GB) is resident in HBM and larger than L2, so no L2 flush is needed.
+The timed iterations replay a CUDA graph of the iteration captured in the
+warm-up (``--no-graph``: kernel by kernel); per-phase times come from K
+further iterations launched kernel by kernel with phase events.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl {tups,reference}]
 
@@ -237,11 +240,12 @@ def run_tups(args, wl_name: str, wl: dict):
     if args.bse_slices:
         sol.set_bse_precision(args.bse_slices)
     K, W = args.steps, args.warmup
+    # iterations replay a captured CUDA graph (captured in the warm-up)
+    sol.set_graph(not args.no_graph)
     for ite in range(W):
         sol.iteration(ite)
     sol.synchronize()
     # ---- timed region: K iterations, device-resident state ----
-    sol.set_timing(True)
     l0 = sol.kernel_launches
     replicas.barrier(ranks)
     torch.cuda.synchronize(device)
@@ -258,8 +262,6 @@ def run_tups(args, wl_name: str, wl: dict):
     torch.cuda.synchronize(device)
     clk = clocks.stop()
     launches = sol.kernel_launches - l0
-    phases = sol.phase_times()
-    sol.set_timing(False)
     # ---- e2e: Sigma from pinned host, one iteration, Sigma back to pinned host ----
     nt = sol.Nt
     h_in = torch.empty(2 * nt, dtype=torch.float64, pin_memory=True).numpy().view(np.complex128)
@@ -275,6 +277,12 @@ def run_tups(args, wl_name: str, wl: dict):
         h_in[:] = h_out
     sol.record_event(3)
     ms_e2e = sol.event_elapsed_ms(2, 3)
+    # ---- per-phase device times (events around each phase; no graph) ----
+    sol.set_timing(True)
+    for k in range(K):
+        sol.iteration(W + 2 * K + k)
+    phases = sol.phase_times()
+    sol.set_timing(False)
     # ---- max over ranks ----
     ms, ms_e2e = replicas.max_over_ranks(ranks, [ms, ms_e2e])
     value = replicas.seconds_per_iteration(ms, K, ws)
@@ -346,6 +354,8 @@ def run_tups(args, wl_name: str, wl: dict):
             "roofline": roof,
             "kernels": kern,
             "phase_ms_per_iter": {p: v[0] / K for p, v in phases.items()},
+            "phase_note": "per-phase CUDA-event times from K further iterations launched kernel by kernel",
+            "launch_mode": "kernel by kernel" if args.no_graph else "CUDA graph per iteration (captured in warm-up)",
             "e2e": {"value": e2e_value, "unit": "s/iter", "h2d_bytes_per_step": 16 * nt,
                     "d2h_bytes_per_step": 16 * nt + 2 * 16 * 8,
                     "api": "Solver.set_sigma_from(pinned) + Solver.iteration + Solver.get_sigma_into(pinned)"},
@@ -551,6 +561,7 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS) + [LU_WORKLOAD], default=DEFAULT_WORKLOAD)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-split", action="store_true", help="skip the split-precision iterations")
+    ap.add_argument("--no-graph", action="store_true", help="launch the timed iterations kernel by kernel")
     ap.add_argument("--bse-slices", type=int, default=0,
                     help="BSE GEMM of the main timed region on this many int8 slices (0 = FP64)")
     ap.add_argument("--no-convergence", action="store_true", help="skip the runs to convergence")
