@@ -533,24 +533,8 @@ extern "C" int tups_set_vertex(tups_ctx* ctx, int channel, int which, const doub
 }
 extern "C" int tups_get_PhiR(tups_ctx* ctx, int channel, double* h) {
   if (!ctx || channel < 0 || channel > 3) return TUPS_ERR_BADARG;
-  if (!h) return tups::set_error(ctx, TUPS_ERR_BADARG, "NULL host buffer");
   const auto& d = ctx->d;
-  // device layout (l_i + Nl l_j, nu_i, nu_j, w, R) -> the reference's (i + Nz j, w, R)
-  const size_t nl2 = (size_t)d.Nl * d.Nl, nf2 = (size_t)d.Nf * d.Nf, n2 = (size_t)d.Nz * d.Nz;
-  const size_t slabs = (size_t)(d.Nf / 2) * d.NR;
-  std::vector<cplx> dev(n2 * slabs);
-  TRY(copy_d2h(ctx, dev.data(), ctx->s.PhiR[channel], dev.size() * sizeof(cplx)));
-  cplx* out = reinterpret_cast<cplx*>(h);
-  for (size_t w = 0; w < slabs; w++)
-    for (int lj = 0; lj < d.Nl; lj++)
-      for (int nj = 0; nj < d.Nf; nj++)
-        for (int li = 0; li < d.Nl; li++)
-          for (int ni = 0; ni < d.Nf; ni++) {
-            const size_t src = (size_t)(li + d.Nl * lj) + nl2 * ((size_t)ni + (size_t)d.Nf * nj + nf2 * w);
-            const size_t dst = (size_t)(li * d.Nf + ni) + (size_t)d.Nz * (lj * d.Nf + nj) + n2 * w;
-            out[dst] = dev[src];
-          }
-  return TUPS_OK;
+  return copy_d2h(ctx, h, ctx->s.PhiR[channel], (size_t)d.Nz * d.Nz * (d.Nf / 2) * d.NR * sizeof(cplx));
 }
 extern "C" int tups_get_M(tups_ctx* ctx, int which, double* h) {
   if (!ctx || which < 0 || which > 3 || !h) return TUPS_ERR_BADARG;

@@ -111,16 +111,10 @@ __device__ __forceinline__ void dmma_16x8x8(double* c, const double* a, const do
       : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
 
-#ifndef PAE_BK_BYTES_K
-#define PAE_BK_BYTES_K 16
-#endif
-#ifndef PAE_MIN_BLOCKS
-#define PAE_MIN_BLOCKS 3
-#endif
 constexpr int PAE_E = 32;          // listed elements per CTA
 constexpr int PAE_ROWS = 2 * PAE_E;  // (target, element) rows
-constexpr int PAE_BK = PAE_BK_BYTES_K;  // K per pipeline step
-constexpr int PAE_LDA = PAE_ROWS + 1;  // 16-byte rows: conflict-free stores of 16 consecutive k
+constexpr int PAE_BK = 16;
+constexpr int PAE_LDA = PAE_ROWS + 2;
 constexpr int PAE_LDB = PAE_BK + 4;
 
 // Element lists: for target pair p, family f and bosonic index W the
@@ -153,7 +147,7 @@ __global__ void k_pae_base(PaePtrs P, const int* __restrict__ ibz, int Nz, int N
 // and F_target += C / Nx.  Warps: 4 along rows (16 rows each) x WN along
 // the (l1,l2) columns, TN n8 tiles each; BN = 8 TN WN >= Nl^2 (or a chunk).
 template <int TN, int WN>
-__global__ void __launch_bounds__(128 * WN, WN == 2 && TN <= 2 ? PAE_MIN_BLOCKS : 1)
+__global__ void __launch_bounds__(128 * WN, WN == 2 && TN <= 2 ? 3 : 1)
     k_pae_mma(PaePtrs P, const int4* __restrict__ elems, const int* __restrict__ counts,
               const int* __restrict__ ibz, const int* __restrict__ signs, int Nz, int Nf, int Nl, int NIBZ, int NR,
               int nchunks, int fam, double inv_nx) {
@@ -207,27 +201,24 @@ __global__ void __launch_bounds__(128 * WN, WN == 2 && TN <= 2 ? PAE_MIN_BLOCKS 
   const cplx* Mf = P.M[pair == 0 ? (fam == 0 ? 0 : 1) : (fam == 0 ? 3 : 2)];
   __syncthreads();
 
-  // gather of one K step into registers: thread -> (element, kk) pairs with
-  // kk fastest, so a half-warp reads consecutive (l3, l4) entries of one
-  // element: Phi(R) is stored (l3 + Nl l4, a, b, w2, R)
+  // gather of one K step into registers: thread -> (element, kk) pairs
   constexpr int APER = PAE_E * PAE_BK / NT > 0 ? PAE_E * PAE_BK / NT : 1;
   cplx ra[APER], rb[APER];
-  const size_t nf2 = (size_t)Nf * Nf;
   auto gather = [&](int kt) {
 #pragma unroll
     for (int i = 0; i < APER; i++) {
       const int p = tid + i * NT;
       ra[i] = rb[i] = cmk(0.0, 0.0);
       if (p >= PAE_E * PAE_BK) continue;
-      const int kk = p % PAE_BK, e = p / PAE_BK;
+      const int e = p % PAE_E, kk = p / PAE_E;
       const int k = kt * PAE_BK + kk;
       if (k >= K) continue;
       const int w2 = e_w2[e];
       if (w2 == 0) continue;
       const int l34 = k % nl2, R = k / nl2;
       const int l3 = l34 % Nl, l4 = l34 / Nl;
-      const size_t xi = (size_t)l34 + (size_t)nl2 * ((size_t)(e_a[e] - 1) + (size_t)Nf * (e_b[e] - 1) +
-                                                      nf2 * ((size_t)(w2 - 1) + (size_t)nh * R));
+      const size_t xi = (size_t)(l3 * Nf + e_a[e] - 1) + (size_t)Nz * (l4 * Nf + e_b[e] - 1) +
+                        n2 * ((size_t)(w2 - 1) + (size_t)nh * R);
       cplx x0 = __ldg(P.PhiR[src0] + xi), x1 = __ldg(P.PhiR[src0 + 1] + xi);
       if (e_tr[e]) {
         const double sg = s_sg[l3] * s_sg[l4];
@@ -244,7 +235,7 @@ __global__ void __launch_bounds__(128 * WN, WN == 2 && TN <= 2 ? PAE_MIN_BLOCKS 
     for (int i = 0; i < APER; i++) {
       const int p = tid + i * NT;
       if (p >= PAE_E * PAE_BK) continue;
-      const int kk = p % PAE_BK, e = p / PAE_BK;
+      const int e = p % PAE_E, kk = p / PAE_E;
       dA[kk * PAE_LDA + e] = ra[i];
       dA[kk * PAE_LDA + PAE_E + e] = rb[i];
     }

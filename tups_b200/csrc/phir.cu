@@ -46,12 +46,8 @@ __global__ void k_phir(PhirPtrs P, const cplx* __restrict__ expSqR, const int* _
         if (R < NR) acc[R] = cfma(v, expSqR[Q + (size_t)NIBZ * (R + (size_t)NR * s)], acc[R]);
     }
   }
-  // layout with the form-factor pair fastest, (l_i + Nl l_j, nu_i, nu_j, w, R):
-  // the crossing kernel gathers Nl^2 consecutive entries per element
   cplx* out = P.PhiR[r];
-  const size_t nl2 = (size_t)Nl * Nl, nf2 = (size_t)Nf * Nf;
-  const size_t base = (size_t)(li + Nl * lj) + nl2 * ((size_t)ni + (size_t)Nf * nj);
-  for (int R = 0; R < NR; R++) out[base + nl2 * nf2 * ((size_t)w + (size_t)nh * R)] = cscale(acc[R], inv_nx);
+  for (int R = 0; R < NR; R++) out[e + n2 * ((size_t)w + (size_t)nh * R)] = cscale(acc[R], inv_nx);
 }
 
 // Crossing tensors per IBZ momentum Q; layout (Nl^4, NIBZ, NR) with l1 fastest.
