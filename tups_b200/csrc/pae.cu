@@ -111,10 +111,10 @@ __device__ __forceinline__ void dmma_16x8x8(double* c, const double* a, const do
       : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
 
-constexpr int PAE_E = 32;          // listed elements per CTA
-constexpr int PAE_ROWS = 2 * PAE_E;  // (target, element) rows
+#ifndef PAE_MIN_BLOCKS
+#define PAE_MIN_BLOCKS 3  // CTAs per SM asked of ptxas for the 8-warp, <= 2 n-tile configs
+#endif
 constexpr int PAE_BK = 16;
-constexpr int PAE_LDA = PAE_ROWS + 2;
 constexpr int PAE_LDB = PAE_BK + 4;
 
 // Element lists: for target pair p, family f and bosonic index W the
@@ -146,13 +146,15 @@ __global__ void k_pae_base(PaePtrs P, const int* __restrict__ ibz, int Nz, int N
 // one family: C^T[(target, element), (l1,l2)] = X^T[(target, element), (l3,l4,R)] M^T
 // and F_target += C / Nx.  Warps: 4 along rows (16 rows each) x WN along
 // the (l1,l2) columns, TN n8 tiles each; BN = 8 TN WN >= Nl^2 (or a chunk).
-template <int TN, int WN>
-__global__ void __launch_bounds__(128 * WN, WN == 2 && TN <= 2 ? 3 : 1)
+template <int TN, int WN, int RW>
+__global__ void __launch_bounds__(32 * RW * WN, RW * WN == 8 && TN <= 2 ? PAE_MIN_BLOCKS : 1)
     k_pae_mma(PaePtrs P, const int4* __restrict__ elems, const int* __restrict__ counts,
               const int* __restrict__ ibz, const int* __restrict__ signs, int Nz, int Nf, int Nl, int NIBZ, int NR,
               int nchunks, int fam, double inv_nx) {
   constexpr int BN = 8 * TN * WN;
-  constexpr int NT = 128 * WN;
+  constexpr int NT = 32 * RW * WN;
+  constexpr int PAE_E = 8 * RW;           // listed elements per CTA
+  constexpr int PAE_LDA = 2 * PAE_E + 2;  // (target, element) rows + pad
   extern __shared__ __align__(16) unsigned char smraw[];
   cplx* sA = reinterpret_cast<cplx*>(smraw);      // [2][BK][LDA]
   cplx* sB = sA + 2 * PAE_BK * PAE_LDA;           // [2][BN][LDB]
@@ -258,7 +260,7 @@ __global__ void __launch_bounds__(128 * WN, WN == 2 && TN <= 2 ? 3 : 1)
   };
 
   const int lane = tid & 31, warp = tid >> 5;
-  const int wr = warp % 4, wc = warp / 4;
+  const int wr = warp % RW, wc = warp / RW;
   const int gid = lane >> 2, tig = lane & 3;
   double cre[TN][4], cim[TN][4];
 #pragma unroll
@@ -325,20 +327,23 @@ __global__ void __launch_bounds__(128 * WN, WN == 2 && TN <= 2 ? 3 : 1)
     }
 }
 
-template <int TN, int WN>
-static int run_pae(tups_ctx* ctx, const PaePtrs& P, int nchunks, int fam, int max_tiles) {
+template <int TN, int WN, int RW>
+static int run_pae(tups_ctx* ctx, const PaePtrs& P, int nchunks, int fam, int max_count) {
   const auto& d = ctx->d;
   constexpr int BN = 8 * TN * WN;
-  const size_t sm = (size_t)(2 * PAE_BK * PAE_LDA + 2 * BN * PAE_LDB) * sizeof(cplx);
-  auto kern = k_pae_mma<TN, WN>;
+  constexpr int E = 8 * RW;
+  constexpr int LDA = 2 * E + 2;
+  const size_t sm = (size_t)(2 * PAE_BK * LDA + 2 * BN * PAE_LDB) * sizeof(cplx);
+  auto kern = k_pae_mma<TN, WN, RW>;
   if (sm > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return cuda_check(ctx, e, "k_pae_mma smem attribute");
   }
+  const int max_tiles = (max_count + E - 1) / E;
   if (max_tiles == 0) return TUPS_OK;
   dim3 grid(max_tiles, 2 * nchunks, d.Nb);
-  kern<<<grid, 128 * WN, sm, ctx->stream>>>(P, ctx->t.pae_elems, ctx->t.pae_counts, ctx->t.ibz, ctx->t.signs, d.Nz,
-                                            d.Nf, d.Nl, d.NIBZ, d.NR, nchunks, fam, 1.0 / d.Nx);
+  kern<<<grid, 32 * RW * WN, sm, ctx->stream>>>(P, ctx->t.pae_elems, ctx->t.pae_counts, ctx->t.ibz, ctx->t.signs,
+                                                d.Nz, d.Nf, d.Nl, d.NIBZ, d.NR, nchunks, fam, 1.0 / d.Nx);
   return after_launch(ctx, "k_pae_mma");
 }
 
@@ -361,7 +366,7 @@ static int build_pae_lists(tups_ctx* ctx) {
             el[(size_t)L * Nf * Nf + c++] = make_int4(nu1 + 256 * nu2, w2, a, b + 65536 * tr);
           }
         cnt[L] = c;
-        ctx->pae_max_tiles[fam] = std::max(ctx->pae_max_tiles[fam], (c + PAE_E - 1) / PAE_E);
+        ctx->pae_max_tiles[fam] = std::max(ctx->pae_max_tiles[fam], c);  // longest list
       }
   void* pe = nullptr;
   void* pc = nullptr;
@@ -406,10 +411,13 @@ int launch_pae(tups_ctx* ctx) {
   if (rc) return rc;
   const int nl2 = d.Nl * d.Nl;
   for (int fam = 0; fam < 2; fam++) {
-    const int mt = ctx->pae_max_tiles[fam];
-    if (nl2 <= 8) rc = run_pae<1, 1>(ctx, P, 1, fam, mt);
-    else if (nl2 <= 32) rc = run_pae<2, 2>(ctx, P, 1, fam, mt);
-    else rc = run_pae<6, 2>(ctx, P, (nl2 + 95) / 96, fam, mt);
+    const int mc = ctx->pae_max_tiles[fam];
+    // tile configs measured on a B200: 8 warps x 32 elements at Nl^2 <= 32
+    // (8x8 / Nl = 5: 2.0 ms against 2.7 ms with 64 elements), 16 warps x 64
+    // elements beyond (16x16 / Nl = 9: 598 ms against 753 ms with 32)
+    if (nl2 <= 8) rc = run_pae<1, 1, 4>(ctx, P, 1, fam, mc);
+    else if (nl2 <= 32) rc = run_pae<2, 2, 4>(ctx, P, 1, fam, mc);
+    else rc = run_pae<6, 2, 8>(ctx, P, (nl2 + 95) / 96, fam, mc);
     if (rc) return rc;
   }
   return TUPS_OK;

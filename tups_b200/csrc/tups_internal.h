@@ -114,7 +114,7 @@ struct tups_ctx {
   // host copies of small state
   double F_max_prev[4] = {0, 0, 0, 0};
   bool have_exp = false, have_M = false, have_phir = false, have_green = false;
-  int pae_max_tiles[2] = {0, 0};  // CTAs along the element lists of each family
+  int pae_max_tiles[2] = {0, 0};  // longest element list of each family
   tups::DeviceTables t;
   tups::DeviceState s;
   tups::ReadoutBufs rd;
