@@ -21,8 +21,7 @@ struct BsePtrs {
 // A = Gamma chi and B = chi Gamma for the instances (q, r) of one chunk;
 // instance = (q - q_begin) * 4 + r.  Column-major (Nz, Nz), row = l*Nf + nu.
 __global__ void k_bse_prep(BsePtrs P, const cplx* __restrict__ chi_ph, const cplx* __restrict__ chi_pp,
-                           cplx* __restrict__ A, cplx* __restrict__ B, int q_begin, int Nz, int Nf, int Nl,
-                           int want_b) {
+                           cplx* __restrict__ A, cplx* __restrict__ B, int q_begin, int Nz, int Nf, int Nl) {
   const int inst = blockIdx.y;
   const int q = q_begin + inst / 4, r = inst % 4;
   const cplx* chi = (r < 2 ? chi_ph : chi_pp) + (size_t)Nl * Nl * Nf * q;
@@ -41,7 +40,7 @@ __global__ void k_bse_prep(BsePtrs P, const cplx* __restrict__ chi_ph, const cpl
       Ai[e] = acc;
     }
     // B[(l1, nu), col] = sum_l2 chi[l1, l2, nu] Gamma[(l2, nu), col]
-    if (want_b) {
+    {
       int l1 = row / Nf, nu = row % Nf;
       cplx acc = cmk(0.0, 0.0);
       for (int l2 = 0; l2 < Nl; l2++)
@@ -290,28 +289,25 @@ static int run_split(tups_ctx* ctx, const BsePtrs& P, int q_begin, int q_count, 
     R.N = Nz;
     R.s = slices;
     const int qb = q_begin + i0 / 4;
-    // rows of [Gamma chi | F] from k_bse_prep's Gamma chi and F_r; columns of
-    // [F ; chi Gamma] with chi Gamma formed while splitting (a warp holds one
-    // column of Gamma in L1)
+    // [Gamma chi | F] and [F ; chi Gamma] from k_bse_prep's products and F_r
     OzOperand A{}, B{};
-    A.mode = 0;
     A.p1 = ctx->s.bse_A + (size_t)Nz * Nz * i0;
     A.s1 = (long long)Nz * Nz;
     A.ld1 = Nz;
+    A.K1 = Nz;
     A.bse2 = 1;
     A.ld2 = Nz;
-    B.mode = 2;
-    A.K1 = A.K2 = B.K1 = B.K2 = Nz;
-    for (int r = 0; r < 4; r++) {
-      A.F[r] = B.F[r] = P.F[r];
-      A.G[r] = B.G[r] = P.G[r];
-    }
-    A.chi_ph = B.chi_ph = ctx->s.chi_ph;
-    A.chi_pp = B.chi_pp = ctx->s.chi_pp;
+    A.K2 = Nz;
+    B.bse1 = 1;
+    B.ld1 = Nz;
+    B.K1 = Nz;
+    B.p2 = ctx->s.bse_B + (size_t)Nz * Nz * i0;
+    B.s2 = (long long)Nz * Nz;
+    B.ld2 = Nz;
+    B.K2 = Nz;
+    for (int r = 0; r < 4; r++) A.F[r] = B.F[r] = P.F[r];
     A.q_begin = B.q_begin = qb;
     A.Nz = B.Nz = Nz;
-    A.Nf = B.Nf = ctx->d.Nf;
-    A.Nl = B.Nl = ctx->d.Nl;
     R.A = A;
     R.B = B;
     oz_bind_work(R, oz_work_layout(nb, Nz, Nz, 2 * Nz, slices), ctx->oz_work);
@@ -345,9 +341,8 @@ int launch_bse_chunk(tups_ctx* ctx, int q_begin, int q_count) {
   const size_t n2 = (size_t)d.Nz * d.Nz;
   dim3 pgrid((unsigned)std::min<size_t>(cdiv(n2, 256), 4096), 4 * q_count);
   phase_begin(ctx, TUPS_PHASE_BSE_PREP);
-  // split precision forms chi Gamma inside its column splitter
   k_bse_prep<<<pgrid, 256, 0, ctx->stream>>>(P, ctx->s.chi_ph, ctx->s.chi_pp, ctx->s.bse_A, ctx->s.bse_B, q_begin,
-                                             d.Nz, d.Nf, d.Nl, slices > 0 ? 0 : 1);
+                                             d.Nz, d.Nf, d.Nl);
   int rc = after_launch(ctx, "k_bse_prep");
   phase_end(ctx, TUPS_PHASE_BSE_PREP);
   if (rc) return rc;

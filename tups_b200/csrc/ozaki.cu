@@ -52,32 +52,15 @@ struct OzLine {
   const cplx* p1;
   const cplx* p2;
   int ld1, ld2, K1;
-  const cplx* G;
-  const cplx* F;
-  const cplx* chi;
-  int Nz, Nf, Nl, mode;
 };
 
 __device__ __forceinline__ OzLine oz_view(const OzOperand& o, int inst) {
   OzLine v;
-  v.mode = o.mode;
   v.ld1 = o.ld1;
   v.ld2 = o.ld2;
   v.K1 = o.K1;
-  v.Nz = o.Nz;
-  v.Nf = o.Nf;
-  v.Nl = o.Nl;
-  v.p1 = v.p2 = v.G = v.F = v.chi = nullptr;
-  if (o.mode == 0) {
-    v.p1 = oz_part(o, 1, inst);
-    v.p2 = o.K2 ? oz_part(o, 2, inst) : nullptr;
-  } else {
-    const int q = o.q_begin + inst / 4, r = inst % 4;
-    const size_t off = (size_t)o.Nz * o.Nz * q;
-    v.G = o.G[r] + off;
-    v.F = o.F[r] + off;
-    v.chi = (r < 2 ? o.chi_ph : o.chi_pp) + (size_t)o.Nl * o.Nl * o.Nf * q;
-  }
+  v.p1 = oz_part(o, 1, inst);
+  v.p2 = o.K2 ? oz_part(o, 2, inst) : nullptr;
   return v;
 }
 
@@ -187,44 +170,21 @@ __global__ void __launch_bounds__(256) k_oz_split_rows(OzOperand A, int M, int s
   }
 }
 
-// Columns of B': one warp per complex column j of B (K1 + K2 long), staged
-// in shared memory (mode 2 also stages the Gamma column and forms chi Gamma
-// from it); writes rows 2j and 2j+1 of every slice.  out: [inst][s][2N][Kpad].
-__global__ void __launch_bounds__(128) k_oz_split_cols(OzOperand B, int N, int s, int Kpad, int8_t* __restrict__ out,
+// Columns of B': one warp per complex column j of B (K1 + K2 long); writes
+// rows 2j and 2j+1 of every slice.  out: [inst][s][2N][Kpad].
+__global__ void __launch_bounds__(256) k_oz_split_cols(OzOperand B, int N, int s, int Kpad, int8_t* __restrict__ out,
                                                        double* __restrict__ cscale) {
-  extern __shared__ __align__(16) unsigned char oz_cols_sm[];
   const int inst = blockIdx.y;
-  const int wib = threadIdx.x >> 5, wpb = blockDim.x >> 5;
-  const int j = blockIdx.x * wpb + wib;
+  const int j = blockIdx.x * 8 + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   if (j >= N) return;
   const int Kc = B.K1 + B.K2;
-  const int gz = B.mode == 2 ? B.Nz : 0;
-  cplx* col = reinterpret_cast<cplx*>(oz_cols_sm) + (size_t)wib * (Kc + gz);
-  cplx* gcol = col + Kc;
   const OzLine V = oz_view(B, inst);
-  if (B.mode == 2) {
-    for (int k = lane; k < B.Nz; k += 32) gcol[k] = V.G[k + (size_t)B.Nz * j];
-    __syncwarp();
-    for (int k = lane; k < Kc; k += 32) {
-      cplx v;
-      if (k < B.Nz) {
-        v = V.F[k + (size_t)B.Nz * j];
-      } else {
-        // (chi Gamma)[(l1, nu), j], summed in the order of k_bse_prep
-        const int kk = k - B.Nz, l1 = kk / B.Nf, nu = kk % B.Nf;
-        v = cmk(0.0, 0.0);
-        for (int l2 = 0; l2 < B.Nl; l2++)
-          v = cfma(__ldg(V.chi + l1 + B.Nl * (l2 + (size_t)B.Nl * nu)), gcol[l2 * B.Nf + nu], v);
-      }
-      col[k] = v;
-    }
-  } else {
-    for (int k = lane; k < Kc; k += 32) col[k] = oz_b(V, k, j);
-  }
-  __syncwarp();
   double mx = 0.0;
-  for (int k = lane; k < Kc; k += 32) mx = fmax(mx, fmax(fabs(col[k].x), fabs(col[k].y)));
+  for (int k = lane; k < Kc; k += 32) {
+    const cplx v = oz_b(V, k, j);
+    mx = fmax(mx, fmax(fabs(v.x), fabs(v.y)));
+  }
   mx = warp_max(mx);
   const int e = oz_exponent(mx);
   if (lane == 0) cscale[(size_t)inst * N + j] = ldexp(1.0, e);
@@ -234,7 +194,7 @@ __global__ void __launch_bounds__(128) k_oz_split_cols(OzOperand B, int N, int s
   for (int k = lane * 4; k < Kc; k += 128) {
     int8_t re[4][8], im[4][8];
     for (int c = 0; c < 4; c++) {
-      const cplx v = k + c < Kc ? col[k + c] : cmk(0.0, 0.0);
+      const cplx v = k + c < Kc ? oz_b(V, k + c, j) : cmk(0.0, 0.0);
       oz_cut(v.x, e, s, &re[c][0], 1);
       oz_cut(v.y, e, s, &im[c][0], 1);
     }
@@ -703,16 +663,8 @@ int oz_run(OzRun& R, cudaStream_t stream, long long* launches) {
     dim3 g((M + 31) / 32, batch);
     k_oz_split_rows<<<g, 256, 0, stream>>>(R.A, M, s, Kpad, R.a_slices, R.rscale);
     if (launches) (*launches)++;
-    // column splitter: up to 4 warps per CTA, one staged column each
-    const size_t per_warp = (size_t)(K + (R.B.mode == 2 ? R.B.Nz : 0)) * sizeof(cplx);
-    const int wpb = (int)std::max<size_t>(1, std::min<size_t>(4, (200 * 1024) / per_warp));
-    if (per_warp > 200 * 1024) return TUPS_ERR_BADDIM;
-    const size_t csm = per_warp * wpb;
-    if (csm > 48 * 1024 &&
-        cudaFuncSetAttribute(k_oz_split_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm) != cudaSuccess)
-      return TUPS_ERR_CUDA;
-    dim3 gc((N + wpb - 1) / wpb, batch);
-    k_oz_split_cols<<<gc, 32 * wpb, csm, stream>>>(R.B, N, s, Kpad, R.b_slices, R.cscale);
+    dim3 gc((N + 7) / 8, batch);
+    k_oz_split_cols<<<gc, 256, 0, stream>>>(R.B, N, s, Kpad, R.b_slices, R.cscale);
     if (launches) (*launches)++;
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return TUPS_ERR_CUDA;

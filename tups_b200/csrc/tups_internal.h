@@ -179,14 +179,6 @@ struct OzOperand {
   int bse1;           // 1: part 1 is F_r(q)
   const cplx* F[4];
   int q_begin, Nz;
-  // mode 0: the parts above.  mode 2: columns of [F ; chi Gamma] of BSE
-  // instance (q, r), chi Gamma formed on the fly from Gamma_r and chi
-  // (K1 = K2 = Nz)
-  int mode;
-  const cplx* G[4];
-  const cplx* chi_ph;
-  const cplx* chi_pp;
-  int Nf, Nl;
 };
 
 struct OzWork {
