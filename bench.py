@@ -327,7 +327,7 @@ def run_tups(args, wl_name: str, wl: dict):
     if not args.no_split and ws == 1:
         split = split_iterations(params, device, K, W, Nz, Nb, peak64)
         graph = graph_iterations(params, device, K, W)
-        if Nz <= 256 and not args.no_convergence:
+        if (Nz <= 256 or args.convergence) and not args.no_convergence:
             conv = to_convergence(params, device)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -565,6 +565,8 @@ def main():
     ap.add_argument("--bse-slices", type=int, default=0,
                     help="BSE GEMM of the main timed region on this many int8 slices (0 = FP64)")
     ap.add_argument("--no-convergence", action="store_true", help="skip the runs to convergence")
+    ap.add_argument("--convergence", action="store_true",
+                    help="also run the loops to convergence when Nz > 256 (minutes at 16x16)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "tups":
         args.warmup = 3

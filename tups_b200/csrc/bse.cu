@@ -226,9 +226,9 @@ static int run_gemm(tups_ctx* ctx, const BsePtrs& P, int q_begin, int q_count) {
 // relative Sigma change r so that the GEMM error (about 10^(1.1 - 2 s) of
 // max|A| max|B| K) stays two decades below it, s_req = ceil((3.1 - log10 r)/2)
 // (3 before the first conv); the online tuner then takes the faster of FP64
-// and s_req slices, from device times of earlier BSE calls.  Split times not
-// measured yet are predicted from a measured one in proportion to the
-// s (s + 1) / 2 slice products; FP64 is timed on the first call.
+// and s_req slices, from device times of earlier BSE calls.  FP64 is timed on
+// the first call; a slice count is tried once unless a smaller one already
+// proved no faster than FP64 (the cost grows with s).
 int current_bse_slices(const tups_ctx* ctx) {
   if (!ctx->precision_ladder) return ctx->bse_slices;
   const double* tms = ctx->use_graph ? ctx->tune_graph_ms : ctx->tune_ms;
@@ -238,15 +238,12 @@ int current_bse_slices(const tups_ctx* ctx) {
   else if (r > 0.0) s_req = std::max(2, (int)std::ceil((3.1 - std::log10(r)) / 2.0));
   if (s_req > 8) return 0;
   if (tms[0] < 0.0) return 0;
-  double est = tms[s_req];
-  if (est < 0.0) {
-    int s0 = -1;
-    for (int s = 2; s <= 8; s++)
-      if (tms[s] >= 0.0 && (s0 < 0 || std::abs(s - s_req) < std::abs(s0 - s_req))) s0 = s;
-    if (s0 < 0) return s_req;  // nothing measured yet: try it
-    est = tms[s0] * (double)(s_req * (s_req + 1)) / (double)(s0 * (s0 + 1));
-  }
-  return est < tms[0] ? s_req : 0;
+  if (tms[s_req] >= 0.0) return tms[s_req] < tms[0] ? s_req : 0;
+  // not measured yet: the cost grows with s, so a measured s' <= s_req that
+  // was no faster than FP64 rules s_req out; otherwise try it once
+  for (int s = 2; s < s_req; s++)
+    if (tms[s] >= 0.0 && tms[s] >= tms[0]) return 0;
+  return s_req;
 }
 
 void bse_tune_collect(tups_ctx* ctx) {
