@@ -327,8 +327,8 @@ def run_tups(args, wl_name: str, wl: dict):
     if not args.no_split and ws == 1:
         split = split_iterations(params, device, K, W, Nz, Nb, peak64)
         graph = graph_iterations(params, device, K, W)
-        if (Nz <= 256 or args.convergence) and not args.no_convergence:
-            conv = to_convergence(params, device)
+    if ws == 1 and (Nz <= 256 or args.convergence) and not args.no_convergence:
+        conv = to_convergence(params, device)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         sec = cpu_oracle_seconds_per_iteration(wl)
