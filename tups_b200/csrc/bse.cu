@@ -22,30 +22,46 @@ struct BsePtrs {
 // instance = (q - q_begin) * 4 + r.  Column-major (Nz, Nz), row = l*Nf + nu.
 __global__ void k_bse_prep(BsePtrs P, const cplx* __restrict__ chi_ph, const cplx* __restrict__ chi_pp,
                            cplx* __restrict__ A, cplx* __restrict__ B, int q_begin, int Nz, int Nf, int Nl) {
+  // Each thread owns one (row, nu) line of Gamma chi or one (nu, col) line of
+  // chi Gamma: it loads the Nl entries of Gamma that the line needs once and
+  // forms all Nl outputs from registers (sums in l ascending order).
+  constexpr int LMAX = 16;
   const int inst = blockIdx.y;
   const int q = q_begin + inst / 4, r = inst % 4;
   const cplx* chi = (r < 2 ? chi_ph : chi_pp) + (size_t)Nl * Nl * Nf * q;
   const cplx* Gm = P.G[r] + (size_t)Nz * Nz * q;
   cplx* Ai = A + (size_t)Nz * Nz * inst;
   cplx* Bi = B + (size_t)Nz * Nz * inst;
-  const size_t n2 = (size_t)Nz * Nz;
-  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n2; e += (size_t)gridDim.x * blockDim.x) {
-    int row = (int)(e % Nz), col = (int)(e / Nz);
-    // A[row, (l2, nu)] = sum_l1 Gamma[row, (l1, nu)] chi[l1, l2, nu]
-    {
-      int l2 = col / Nf, nu = col % Nf;
-      cplx acc = cmk(0.0, 0.0);
-      for (int l1 = 0; l1 < Nl; l1++)
-        acc = cfma(Gm[row + (size_t)Nz * (l1 * Nf + nu)], chi[l1 + Nl * (l2 + (size_t)Nl * nu)], acc);
-      Ai[e] = acc;
-    }
-    // B[(l1, nu), col] = sum_l2 chi[l1, l2, nu] Gamma[(l2, nu), col]
-    {
-      int l1 = row / Nf, nu = row % Nf;
-      cplx acc = cmk(0.0, 0.0);
-      for (int l2 = 0; l2 < Nl; l2++)
-        acc = cfma(chi[l1 + Nl * (l2 + (size_t)Nl * nu)], Gm[(l2 * Nf + nu) + (size_t)Nz * col], acc);
-      Bi[e] = acc;
+  const size_t lines = (size_t)Nz * Nf;
+  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < 2 * lines; t += (size_t)gridDim.x * blockDim.x) {
+    cplx g[LMAX];
+    if (t < lines) {
+      // A[row, (l2, nu)] = sum_l1 Gamma[row, (l1, nu)] chi[l1, l2, nu]
+      const int row = (int)(t % Nz), nu = (int)(t / Nz);
+#pragma unroll
+      for (int l = 0; l < LMAX; l++)
+        if (l < Nl) g[l] = Gm[row + (size_t)Nz * (l * Nf + nu)];
+      for (int l2 = 0; l2 < Nl; l2++) {
+        cplx acc = cmk(0.0, 0.0);
+#pragma unroll
+        for (int l1 = 0; l1 < LMAX; l1++)
+          if (l1 < Nl) acc = cfma(g[l1], chi[l1 + Nl * (l2 + (size_t)Nl * nu)], acc);
+        Ai[row + (size_t)Nz * (l2 * Nf + nu)] = acc;
+      }
+    } else {
+      // B[(l1, nu), col] = sum_l2 chi[l1, l2, nu] Gamma[(l2, nu), col]
+      const size_t u = t - lines;
+      const int nu = (int)(u % Nf), col = (int)(u / Nf);
+#pragma unroll
+      for (int l = 0; l < LMAX; l++)
+        if (l < Nl) g[l] = Gm[(l * Nf + nu) + (size_t)Nz * col];
+      for (int l1 = 0; l1 < Nl; l1++) {
+        cplx acc = cmk(0.0, 0.0);
+#pragma unroll
+        for (int l2 = 0; l2 < LMAX; l2++)
+          if (l2 < Nl) acc = cfma(chi[l1 + Nl * (l2 + (size_t)Nl * nu)], g[l2], acc);
+        Bi[(l1 * Nf + nu) + (size_t)Nz * col] = acc;
+      }
     }
   }
 }
@@ -335,8 +351,9 @@ int launch_bse_chunk(tups_ctx* ctx, int q_begin, int q_count) {
     P.scale[r] = c[r] * ctx->p.f_damping * a;
   }
   const int slices = ctx->cur_slices;
-  const size_t n2 = (size_t)d.Nz * d.Nz;
-  dim3 pgrid((unsigned)std::min<size_t>(cdiv(n2, 256), 4096), 4 * q_count);
+  if (d.Nl > 16) return set_error(ctx, TUPS_ERR_BADDIM, "Nl > 16 not supported by k_bse_prep");
+  const size_t lines2 = (size_t)2 * d.Nz * d.Nf;
+  dim3 pgrid((unsigned)std::min<size_t>(cdiv(lines2, 256), 4096), 4 * q_count);
   phase_begin(ctx, TUPS_PHASE_BSE_PREP);
   k_bse_prep<<<pgrid, 256, 0, ctx->stream>>>(P, ctx->s.chi_ph, ctx->s.chi_pp, ctx->s.bse_A, ctx->s.bse_B, q_begin,
                                              d.Nz, d.Nf, d.Nl);
