@@ -163,16 +163,18 @@ __global__ void __launch_bounds__(32 * RW * WN, RW * WN == 8 && TN <= 2 ? PAE_MI
   __shared__ double fac[2][2];
   __shared__ int src0;
 
-  const int pair = blockIdx.y / nchunks, chunk = blockIdx.y % nchunks;
-  // slots ordered with the bosonic frequency outermost, so that the CTAs in
-  // flight share the same band of Phi(R) in L2
-  const int q = (blockIdx.z % NIBZ) * (Nf / 2) + blockIdx.z / NIBZ;
+  // grid (Q, tile x pair x chunk, w): the CTAs in flight are the IBZ momenta of
+  // one element tile, so they gather the same Phi(R) entries (Phi(R) does not
+  // depend on Q) and L2 serves all but the first
+  const int pc = blockIdx.y % (2 * nchunks), tile = blockIdx.y / (2 * nchunks);
+  const int pair = pc / nchunks, chunk = pc % nchunks;
+  const int q = blockIdx.x * (Nf / 2) + blockIdx.z;
   const int W = ibz[3 * q + 2];
   const int Qi = q / (Nf / 2);
   const int nh = Nf / 2;
   const int list = pae_list(pair, fam, W, nh);
   const int cnt = counts[list];
-  const int e0 = blockIdx.x * PAE_E;
+  const int e0 = tile * PAE_E;
   if (e0 >= cnt) return;
   const int nl2 = Nl * Nl, nl4 = nl2 * nl2;
   const int K = nl2 * NR;
@@ -341,7 +343,7 @@ static int run_pae(tups_ctx* ctx, const PaePtrs& P, int nchunks, int fam, int ma
   }
   const int max_tiles = (max_count + E - 1) / E;
   if (max_tiles == 0) return TUPS_OK;
-  dim3 grid(max_tiles, 2 * nchunks, d.Nb);
+  dim3 grid(d.NIBZ, max_tiles * 2 * nchunks, d.Nf / 2);
   kern<<<grid, 32 * RW * WN, sm, ctx->stream>>>(P, ctx->t.pae_elems, ctx->t.pae_counts, ctx->t.ibz, ctx->t.signs,
                                                 d.Nz, d.Nf, d.Nl, d.NIBZ, d.NR, nchunks, fam, 1.0 / d.Nx);
   return after_launch(ctx, "k_pae_mma");
