@@ -367,8 +367,11 @@ int launch_bse_chunk(tups_ctx* ctx, int q_begin, int q_count) {
     return rc;
   }
   phase_begin(ctx, TUPS_PHASE_BSE_GEMM);
-  // tile choice: 64x64 when Nz is a multiple of 64 (or large), else 32x32
-  if (d.Nz % 64 == 0 || d.Nz > 512) rc = run_gemm<64, 64, 16, 2, 2, 3>(ctx, P, q_begin, q_count);
+  // tile choice: 64x64 when Nz is a multiple of 64 (or large), else 32x32;
+  // measured on a B200: 8 warps of 32 x 16 at 64 x 64 (16x16 / Nl = 9:
+  // 541 ms against 574 ms with 4 warps of 32 x 32); 32 x 32 tiles with
+  // 4 warps at Nz = 160 (2.13 ms; 2.4-2.8 ms with 4 stages, BK = 32 or 2 warps)
+  if (d.Nz % 64 == 0 || d.Nz > 512) rc = run_gemm<64, 64, 16, 2, 4, 3>(ctx, P, q_begin, q_count);
   else if (d.Nz >= 32) rc = run_gemm<32, 32, 16, 2, 2, 3>(ctx, P, q_begin, q_count);
   else rc = run_gemm<16, 16, 16, 1, 2, 3>(ctx, P, q_begin, q_count);
   phase_end(ctx, TUPS_PHASE_BSE_GEMM);
