@@ -21,6 +21,20 @@ struct PhirPtrs {
 __global__ void k_phir(PhirPtrs P, const cplx* __restrict__ expSqR, const int* __restrict__ symlist,
                        const int* __restrict__ lsym, const double* __restrict__ lfac, int Nz, int Nf, int Nl,
                        int NIBZ, int NR, double inv_nx) {
+  // the phase tables (expSqR, star lists, l-space maps) of all threads in
+  // shared memory: the inner loop reads only Phi from global memory
+  extern __shared__ __align__(16) unsigned char phir_sm[];
+  cplx* sE = reinterpret_cast<cplx*>(phir_sm);                   // (NIBZ, NR, NS)
+  int* sSym = reinterpret_cast<int*>(sE + (size_t)NIBZ * NR * NS);  // (NS, NIBZ)
+  __shared__ int sL[NS * 16];
+  __shared__ double sF[NS * 16];
+  for (int t = threadIdx.x; t < NIBZ * NR * NS; t += blockDim.x) sE[t] = expSqR[t];
+  for (int t = threadIdx.x; t < NIBZ * NS; t += blockDim.x) sSym[t] = symlist[t];
+  for (int t = threadIdx.x; t < NS * Nl; t += blockDim.x) {
+    sL[t] = lsym[t];
+    sF[t] = lfac[t];
+  }
+  __syncthreads();
   const int r = blockIdx.z;
   const int w = blockIdx.y;  // 0..Nf/2-1
   const size_t n2 = (size_t)Nz * Nz;
@@ -32,18 +46,18 @@ __global__ void k_phir(PhirPtrs P, const cplx* __restrict__ expSqR, const int* _
   cplx acc[8];
 #pragma unroll
   for (int R = 0; R < 8; R++) acc[R] = cmk(0.0, 0.0);
-  const cplx* G = P.G[r];
+  const cplx* G = P.G[r] + n2 * (size_t)w;
   for (int s = 0; s < NS; s++) {
-    const int lis = lsym[s + NS * li], ljs = lsym[s + NS * lj];
-    const double f = lfac[s + NS * li] * lfac[s + NS * lj];
-    const size_t src = (size_t)(lis * Nf + ni) + (size_t)Nz * (ljs * Nf + nj);
+    const int lis = sL[s + NS * li], ljs = sL[s + NS * lj];
+    const double f = sF[s + NS * li] * sF[s + NS * lj];
+    const cplx* src = G + (size_t)(lis * Nf + ni) + (size_t)Nz * (ljs * Nf + nj);
     for (int Q = 0; Q < NIBZ; Q++) {
-      if (!symlist[NS * Q + s]) continue;
-      cplx v = G[src + n2 * ((size_t)Q * nh + w)];
-      v = cscale(v, f);
+      if (!sSym[NS * Q + s]) continue;
+      const cplx v = cscale(__ldg(src + n2 * (size_t)Q * nh), f);
+      const cplx* eq = sE + Q + (size_t)NIBZ * NR * s;
 #pragma unroll
       for (int R = 0; R < 8; R++)
-        if (R < NR) acc[R] = cfma(v, expSqR[Q + (size_t)NIBZ * (R + (size_t)NR * s)], acc[R]);
+        if (R < NR) acc[R] = cfma(v, eq[(size_t)NIBZ * R], acc[R]);
     }
   }
   cplx* out = P.PhiR[r];
@@ -114,10 +128,16 @@ int launch_phir(tups_ctx* ctx) {
     P.PhiR[r] = ctx->s.PhiR[r];
   }
   if (d.NR > 8) return set_error(ctx, TUPS_ERR_BADDIM, "NR > 8 not supported");
+  if (d.Nl > 16) return set_error(ctx, TUPS_ERR_BADDIM, "Nl > 16 not supported by k_phir");
   const size_t n2 = (size_t)d.Nz * d.Nz;
-  dim3 grid(cdiv(n2, 128), d.Nf / 2, 4);
-  k_phir<<<grid, 128, 0, ctx->stream>>>(P, ctx->t.expSqR, ctx->t.symlist, ctx->t.lsym, ctx->t.lfac, d.Nz, d.Nf,
-                                        d.Nl, d.NIBZ, d.NR, 1.0 / d.Nx);
+  const size_t sm = (size_t)d.NIBZ * d.NR * NS * sizeof(cplx) + (size_t)d.NIBZ * NS * sizeof(int);
+  if (sm > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(k_phir, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return cuda_check(ctx, e, "k_phir smem attribute");
+  }
+  dim3 grid(cdiv(n2, 256), d.Nf / 2, 4);
+  k_phir<<<grid, 256, sm, ctx->stream>>>(P, ctx->t.expSqR, ctx->t.symlist, ctx->t.lsym, ctx->t.lfac, d.Nz, d.Nf,
+                                         d.Nl, d.NIBZ, d.NR, 1.0 / d.Nx);
   return after_launch(ctx, "k_phir");
 }
 
