@@ -20,12 +20,13 @@ struct BsePtrs {
 
 // A = Gamma chi and B = chi Gamma for the instances (q, r) of one chunk;
 // instance = (q - q_begin) * 4 + r.  Column-major (Nz, Nz), row = l*Nf + nu.
+// Each thread owns one (row, nu) line of Gamma chi or one (nu, col) line of
+// chi Gamma: it loads the Nl entries of Gamma that the line needs once and
+// forms all Nl outputs from registers (sums in l ascending order).  LMAX >= Nl
+// sizes the register array (instantiated for the shell counts 1, 5, 9, 13).
+template <int LMAX>
 __global__ void k_bse_prep(BsePtrs P, const cplx* __restrict__ chi_ph, const cplx* __restrict__ chi_pp,
                            cplx* __restrict__ A, cplx* __restrict__ B, int q_begin, int Nz, int Nf, int Nl) {
-  // Each thread owns one (row, nu) line of Gamma chi or one (nu, col) line of
-  // chi Gamma: it loads the Nl entries of Gamma that the line needs once and
-  // forms all Nl outputs from registers (sums in l ascending order).
-  constexpr int LMAX = 16;
   const int inst = blockIdx.y;
   const int q = q_begin + inst / 4, r = inst % 4;
   const cplx* chi = (r < 2 ? chi_ph : chi_pp) + (size_t)Nl * Nl * Nf * q;
@@ -355,8 +356,10 @@ int launch_bse_chunk(tups_ctx* ctx, int q_begin, int q_count) {
   const size_t lines2 = (size_t)2 * d.Nz * d.Nf;
   dim3 pgrid((unsigned)std::min<size_t>(cdiv(lines2, 256), 4096), 4 * q_count);
   phase_begin(ctx, TUPS_PHASE_BSE_PREP);
-  k_bse_prep<<<pgrid, 256, 0, ctx->stream>>>(P, ctx->s.chi_ph, ctx->s.chi_pp, ctx->s.bse_A, ctx->s.bse_B, q_begin,
-                                             d.Nz, d.Nf, d.Nl);
+  auto prep = d.Nl <= 1 ? k_bse_prep<1> : d.Nl <= 5 ? k_bse_prep<5> : d.Nl <= 9 ? k_bse_prep<9>
+             : d.Nl <= 13 ? k_bse_prep<13> : k_bse_prep<16>;
+  prep<<<pgrid, 256, 0, ctx->stream>>>(P, ctx->s.chi_ph, ctx->s.chi_pp, ctx->s.bse_A, ctx->s.bse_B, q_begin, d.Nz,
+                                       d.Nf, d.Nl);
   int rc = after_launch(ctx, "k_bse_prep");
   phase_end(ctx, TUPS_PHASE_BSE_PREP);
   if (rc) return rc;
