@@ -92,7 +92,7 @@ __device__ __forceinline__ void dmma16x8x8(double* c, const double* a, const dou
 // Batched complex GEMM on the FP64 tensor cores with the BSE epilogue.
 // CTA tile BM x BN (complex), K step BK; WM x WN warps, warp tile
 // (16 TM) x (8 TN).  Left operand L = [A | F] (Nz x 2Nz), right R = [F ; B].
-template <int BM, int BN, int BK, int WM, int WN, int STAGES>
+template <int BM, int BN, int BK, int WM, int WN, int STAGES, bool M3>
 __global__ void __launch_bounds__(WM* WN * 32) k_bse_gemm(BsePtrs P, const cplx* __restrict__ A,
                                                           const cplx* __restrict__ B, int q_begin, int Nz,
                                                           double one_minus_f) {
@@ -142,13 +142,19 @@ __global__ void __launch_bounds__(WM* WN * 32) k_bse_gemm(BsePtrs P, const cplx*
     }
   };
 
-  double cre[TM][TN][4], cim[TM][TN][4];
+  // M3: three real products per complex one (Gauss): P1 = Ar Br, P2 = Ai Bi,
+  // P3 = (Ar + Ai)(Br + Bi); Re = P1 - P2, Im = P3 - P1 - P2.  Otherwise four:
+  // Re += Ar Br - Ai Bi, Im += Ar Bi + Ai Br (accumulated in p1 = Re, p2 = Im).
+  double p1[TM][TN][4], p2[TM][TN][4], p3[M3 ? TM : 1][M3 ? TN : 1][4];
 #pragma unroll
   for (int i = 0; i < TM; i++)
 #pragma unroll
     for (int j = 0; j < TN; j++)
 #pragma unroll
-      for (int e = 0; e < 4; e++) cre[i][j][e] = cim[i][j][e] = 0.0;
+      for (int e = 0; e < 4; e++) {
+        p1[i][j][e] = p2[i][j][e] = 0.0;
+        if (M3) p3[M3 ? i : 0][M3 ? j : 0][e] = 0.0;
+      }
 
 #pragma unroll
   for (int s = 0; s < STAGES - 1; s++) {
@@ -190,18 +196,53 @@ __global__ void __launch_bounds__(WM* WN * 32) k_bse_gemm(BsePtrs P, const cplx*
         bre[j][0] = w0.x; bim[j][0] = w0.y;
         bre[j][1] = w1.x; bim[j][1] = w1.y;
       }
+      if (M3) {
+        double asum[TM][4], bsum[TN][2];
 #pragma unroll
-      for (int i = 0; i < TM; i++)
+        for (int i = 0; i < TM; i++)
 #pragma unroll
-        for (int j = 0; j < TN; j++) {
-          dmma16x8x8(cre[i][j], are[i], bre[j]);
-          dmma16x8x8(cre[i][j], anim[i], bim[j]);
-          dmma16x8x8(cim[i][j], are[i], bim[j]);
-          dmma16x8x8(cim[i][j], aim[i], bre[j]);
-        }
+          for (int e = 0; e < 4; e++) asum[i][e] = are[i][e] + aim[i][e];
+#pragma unroll
+        for (int j = 0; j < TN; j++)
+#pragma unroll
+          for (int e = 0; e < 2; e++) bsum[j][e] = bre[j][e] + bim[j][e];
+#pragma unroll
+        for (int i = 0; i < TM; i++)
+#pragma unroll
+          for (int j = 0; j < TN; j++) {
+            dmma16x8x8(p1[i][j], are[i], bre[j]);
+            dmma16x8x8(p2[i][j], aim[i], bim[j]);
+            dmma16x8x8(p3[M3 ? i : 0][M3 ? j : 0], asum[i], bsum[j]);
+          }
+      } else {
+#pragma unroll
+        for (int i = 0; i < TM; i++)
+#pragma unroll
+          for (int j = 0; j < TN; j++) {
+            dmma16x8x8(p1[i][j], are[i], bre[j]);
+            dmma16x8x8(p1[i][j], anim[i], bim[j]);
+            dmma16x8x8(p2[i][j], are[i], bim[j]);
+            dmma16x8x8(p2[i][j], aim[i], bre[j]);
+          }
+      }
     }
   }
   cp_async_wait<0>();
+  double cre[TM][TN][4], cim[TM][TN][4];
+#pragma unroll
+  for (int i = 0; i < TM; i++)
+#pragma unroll
+    for (int j = 0; j < TN; j++)
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        if (M3) {
+          cre[i][j][e] = p1[i][j][e] - p2[i][j][e];
+          cim[i][j][e] = p3[M3 ? i : 0][M3 ? j : 0][e] - p1[i][j][e] - p2[i][j][e];
+        } else {
+          cre[i][j][e] = p1[i][j][e];
+          cim[i][j][e] = p2[i][j][e];
+        }
+      }
 
   // epilogue: Phi = s * C + (1-f) (F - Gamma), written over Gamma
   const double s = P.scale[r];
@@ -221,12 +262,12 @@ __global__ void __launch_bounds__(WM* WN * 32) k_bse_gemm(BsePtrs P, const cplx*
       }
 }
 
-template <int BM, int BN, int BK, int WM, int WN, int STAGES>
+template <int BM, int BN, int BK, int WM, int WN, int STAGES, bool M3>
 static int run_gemm(tups_ctx* ctx, const BsePtrs& P, int q_begin, int q_count) {
   const int Nz = ctx->d.Nz;
   constexpr int LDL = BM + 2, LDR = BK + 4;
   size_t sm = (size_t)STAGES * (BK * LDL + BN * LDR) * sizeof(cplx);
-  auto kern = k_bse_gemm<BM, BN, BK, WM, WN, STAGES>;
+  auto kern = k_bse_gemm<BM, BN, BK, WM, WN, STAGES, M3>;
   if (sm > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return cuda_check(ctx, e, "k_bse_gemm smem attribute");
@@ -371,12 +412,14 @@ int launch_bse_chunk(tups_ctx* ctx, int q_begin, int q_count) {
   }
   phase_begin(ctx, TUPS_PHASE_BSE_GEMM);
   // tile choice: 64x64 when Nz is a multiple of 64 (or large), else 32x32;
-  // measured on a B200: 8 warps of 32 x 16 at 64 x 64 (16x16 / Nl = 9:
-  // 541 ms against 574 ms with 4 warps of 32 x 32); 32 x 32 tiles with
-  // 4 warps at Nz = 160 (2.13 ms; 2.4-2.8 ms with 4 stages, BK = 32 or 2 warps)
-  if (d.Nz % 64 == 0 || d.Nz > 512) rc = run_gemm<64, 64, 16, 2, 4, 3>(ctx, P, q_begin, q_count);
-  else if (d.Nz >= 32) rc = run_gemm<32, 32, 16, 2, 2, 3>(ctx, P, q_begin, q_count);
-  else rc = run_gemm<16, 16, 16, 1, 2, 3>(ctx, P, q_begin, q_count);
+  // measured on a B200: 8 warps of 32 x 16 at 64 x 64 with four real
+  // products per complex one (16x16 / Nl = 9: 541 ms against 574 ms with
+  // 4 warps of 32 x 32, 656 ms with three); 32 x 32 tiles with 4 warps and
+  // three real products at Nz = 160 (1.93 ms against 2.13 ms with four;
+  // 2.4-2.8 ms with 4 stages, BK = 32 or 2 warps)
+  if (d.Nz % 64 == 0 || d.Nz > 512) rc = run_gemm<64, 64, 16, 2, 4, 3, false>(ctx, P, q_begin, q_count);
+  else if (d.Nz >= 32) rc = run_gemm<32, 32, 16, 2, 2, 3, true>(ctx, P, q_begin, q_count);
+  else rc = run_gemm<16, 16, 16, 1, 2, 3, true>(ctx, P, q_begin, q_count);
   phase_end(ctx, TUPS_PHASE_BSE_GEMM);
   return rc;
 }
