@@ -58,7 +58,7 @@ typedef struct tups_params {
   int f_range;          /* 10 */
   double f_damping;     /* 11 */
   int ite_max;          /* 12 */
-  int DGA;              /* 13 (must be 0: the DGA input path is not on the hot path) */
+  int DGA;              /* 13: Lambda from fname_L + "_ph.init" / "_pp.init" (SRC/parquet_util.f90:317-346) */
   char fname_L[256];    /* 14 */
   int use_sig_dmft;     /* 15 */
   char fname_sig_dmft[256]; /* 16 */

@@ -477,6 +477,41 @@ def freq(st: State, iw):
     return 1j * (math.pi / st.p.beta * (2.0 * (iw - st.Nf // 2 - 1) + 1.0))
 
 
+def read_lambda_file(path: str, Nf: int) -> tuple[np.ndarray, np.ndarray]:
+    """DGA Lambda input (parquet_util.f90:321-343): records in the order k1
+    (slowest), k2, q (fastest), each a list-directed read of
+    ``i i i re1 im1 re2 im2`` (a record may span lines; items left on its last
+    line are skipped).  Returns the two (Nf, Nf, Nf/2) tables."""
+    A = np.zeros((Nf, Nf, Nf // 2), dtype=np.complex128)
+    B = np.zeros_like(A)
+    with open(path) as fh:
+        lines = iter(fh.read().splitlines())
+        for k1 in range(Nf):
+            for k2 in range(Nf):
+                for q in range(Nf // 2):
+                    tok: list[str] = []
+                    while len(tok) < 7:
+                        tok += next(lines).replace(",", " ").split()
+                    for t in tok[:3]:
+                        int(t)  # integer labels, read and dropped as in the reference
+                    v = [_f_real(t) for t in tok[3:7]]
+                    A[k1, k2, q] = complex(v[0], v[1])
+                    B[k1, k2, q] = complex(v[2], v[3])
+    return A, B
+
+
+def write_lambda_file(path: str, A: np.ndarray, B: np.ndarray) -> None:
+    """Writes two (Nf, Nf, Nf/2) tables in the record order of
+    ``read_lambda_file``, one record per line, 17 significant digits."""
+    Nf = A.shape[0]
+    with open(path, "w") as fh:
+        for k1 in range(Nf):
+            for k2 in range(Nf):
+                for q in range(Nf // 2):
+                    a, b = A[k1, k2, q], B[k1, k2, q]
+                    fh.write(f"{k1 + 1} {k2 + 1} {q + 1} {a.real:.17e} {a.imag:.17e} {b.real:.17e} {b.imag:.17e}\n")
+
+
 def initialize(p: Params) -> State:
     """``set_parameters`` derived sizes (parquet_ini.f90:326-349),
     ``Initialization`` (parquet_util.f90:14-478), ``FF_array`` and the
@@ -485,8 +520,6 @@ def initialize(p: Params) -> State:
         raise ValueError("Nf must be even")
     if p.old or p.SDE_old:
         raise NotImplementedError("old PAE/SDE paths are outside the hot path")
-    if p.DGA:
-        raise NotImplementedError("DGA Lambda input is outside the hot path")
     st = State(p=p)
     st.Nx = st.Ny = p.Nx
     st.Nf = p.Nf
@@ -569,12 +602,18 @@ def initialize(p: Params) -> State:
             rows = [ln.split() for ln in fh.read().splitlines() if ln.strip()]
         sdmft = np.array([complex(0.0, _f_real(r[2])) for r in rows[:Nf]])
         Sigma[:] = np.tile(sdmft, st.Nc)
-    # Lambda (parquet_util.f90:302-314)
+    # Lambda (parquet_util.f90:302-346)
     U = p.U
-    Ls = {"d": np.full((Nf, Nf, Nf // 2), U, dtype=np.complex128),
-          "m": np.full((Nf, Nf, Nf // 2), -U, dtype=np.complex128),
-          "s": np.full((Nf, Nf, Nf // 2), 2.0 * U, dtype=np.complex128),
-          "t": np.zeros((Nf, Nf, Nf // 2), dtype=np.complex128)}
+    if p.DGA:
+        base = p.fname_L.rstrip()
+        Ls = {}
+        Ls["d"], Ls["m"] = read_lambda_file(base + "_ph.init", Nf)
+        Ls["s"], Ls["t"] = read_lambda_file(base + "_pp.init", Nf)
+    else:
+        Ls = {"d": np.full((Nf, Nf, Nf // 2), U, dtype=np.complex128),
+              "m": np.full((Nf, Nf, Nf // 2), -U, dtype=np.complex128),
+              "s": np.full((Nf, Nf, Nf // 2), 2.0 * U, dtype=np.complex128),
+              "t": np.zeros((Nf, Nf, Nf // 2), dtype=np.complex128)}
     st.tables["L"] = Ls
     # vertex init, preprocessing.f90:100-116
     aux = abs(1.0 / (FF[0, 0, 0] * FF[0, 0, 0]))

@@ -81,24 +81,27 @@ __global__ void k_vertex_update(cplx* __restrict__ G0, cplx* __restrict__ G1, cp
     G[i] = csub(F[i], G[i]);
 }
 
-// F = G = value on the (l=1, l=1) nu-block of every slot (SRC/preprocessing.f90:102-116)
-__global__ void k_fill_lambda_block(cplx* __restrict__ F, cplx* __restrict__ G, int Nz, int Nf, int Nb,
-                                    double value) {
+// F = G = aux * Lambda(:, :, w) on the (l=1, l=1) nu-block of every slot, w
+// the slot's bosonic index (SRC/preprocessing.f90:102-116)
+__global__ void k_fill_lambda_block(cplx* __restrict__ F, cplx* __restrict__ G, const cplx* __restrict__ L,
+                                    const int* __restrict__ ibz, int Nz, int Nf, int Nb, double aux) {
   const size_t n = (size_t)Nf * Nf * Nb;
   for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
     const int i = (int)(e % Nf), j = (int)((e / Nf) % Nf);
     const size_t q = e / ((size_t)Nf * Nf);
+    const int w = ibz[3 * q + 2];
+    const cplx l = L[i + (size_t)Nf * (j + (size_t)Nf * (w - 1))];
     const size_t idx = i + (size_t)Nz * (j + (size_t)Nz * q);
-    F[idx] = cmk(value, 0.0);
-    G[idx] = cmk(value, 0.0);
+    F[idx] = cmk(l.x * aux, l.y * aux);
+    G[idx] = cmk(l.x * aux, l.y * aux);
   }
 }
 
-int launch_fill_lambda_block(tups_ctx* ctx, cplx* F, cplx* G, double value) {
+int launch_fill_lambda_block(tups_ctx* ctx, cplx* F, cplx* G, const cplx* L, double aux) {
   const auto& d = ctx->d;
   const size_t n = (size_t)d.Nf * d.Nf * d.Nb;
-  k_fill_lambda_block<<<(unsigned)std::min<size_t>(cdiv(n, 256), 148 * 8), 256, 0, ctx->stream>>>(F, G, d.Nz, d.Nf,
-                                                                                                d.Nb, value);
+  k_fill_lambda_block<<<(unsigned)std::min<size_t>(cdiv(n, 256), 148 * 8), 256, 0, ctx->stream>>>(
+      F, G, L, ctx->t.ibz, d.Nz, d.Nf, d.Nb, aux);
   return after_launch(ctx, "k_fill_lambda_block");
 }
 

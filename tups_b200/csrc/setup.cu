@@ -425,7 +425,6 @@ static int build_tables(tups_ctx* ctx) {
   if (p.Ngrain < 1) return tups::set_error(ctx, TUPS_ERR_BADDIM, "Ngrain must be >= 1");
   if (p.f_range < 0) return tups::set_error(ctx, TUPS_ERR_BADDIM, "f_range must be >= 0");
   if (p.old || p.SDE_old) return tups::set_error(ctx, TUPS_ERR_BADARG, "old PAE/SDE paths are not supported");
-  if (p.DGA) return tups::set_error(ctx, TUPS_ERR_BADARG, "DGA input is not supported");
   d.Nx = d.Ny = p.Nx;
   d.Nf = p.Nf;
   d.Ngrain = p.Ngrain;
@@ -527,6 +526,51 @@ static int build_tables(tups_ctx* ctx) {
   return TUPS_OK;
 }
 
+// Fortran character variables are blank-padded: TRIM drops trailing blanks
+static std::string trim_name(const char* c) {
+  std::string t(c);
+  while (!t.empty() && (t.back() == ' ' || t.back() == '\t')) t.pop_back();
+  return t;
+}
+
+// DGA Lambda file (SRC/parquet_util.f90:321-343): Nf * Nf * Nf/2 records in
+// the order k1 (slowest), k2, q (fastest), each read list-directed as
+// "i i i re1 im1 re2 im2": a record may span lines, items left on its last
+// line are skipped, commas separate like blanks.  The first complex number
+// goes to A(k1, k2, q) (Lambda_d or Lambda_s), the second to B (Lambda_m or
+// Lambda_t), both stored (Nf, Nf, Nf/2) column-major.
+static int read_lambda_file(tups_ctx* ctx, const std::string& path, int Nf, std::vector<cplx>& A,
+                            std::vector<cplx>& B) {
+  std::ifstream in(path);
+  if (!in) return tups::set_error(ctx, TUPS_ERR_IO, "cannot open " + path);
+  const size_t nL = (size_t)Nf * Nf * (Nf / 2);
+  A.assign(nL, make_double2(0.0, 0.0));
+  B.assign(nL, make_double2(0.0, 0.0));
+  std::string line;
+  for (int k1 = 0; k1 < Nf; k1++)
+    for (int k2 = 0; k2 < Nf; k2++)
+      for (int q = 0; q < Nf / 2; q++) {
+        std::vector<std::string> tok;
+        while (tok.size() < 7 && std::getline(in, line)) {
+          for (auto& c : line)
+            if (c == ',') c = ' ';
+          std::istringstream ls(line);
+          std::string x;
+          while (ls >> x) tok.push_back(x);
+        }
+        if (tok.size() < 7) return tups::set_error(ctx, TUPS_ERR_IO, path + ": file too short");
+        int itemp;
+        double v[4];
+        bool ok = parse_int(tok[0], &itemp) && parse_int(tok[1], &itemp) && parse_int(tok[2], &itemp);
+        for (int a = 0; a < 4; a++) ok = ok && parse_real(tok[3 + a], &v[a]);
+        if (!ok) return tups::set_error(ctx, TUPS_ERR_IO, path + ": bad record");
+        const size_t idx = (size_t)k1 + (size_t)Nf * (k2 + (size_t)Nf * q);
+        A[idx] = make_double2(v[0], v[1]);
+        B[idx] = make_double2(v[2], v[3]);
+      }
+  return TUPS_OK;
+}
+
 static int upload_tables(tups_ctx* ctx) {
   const tups_dims& d = ctx->d;
   auto& t = ctx->t;
@@ -541,14 +585,20 @@ static int upload_tables(tups_ctx* ctx) {
   TRY(upload(ctx, &t.ibz, ctx->ibz));
   TRY(upload(ctx, &t.symlist, ctx->symlist));
   TRY(upload(ctx, &t.symq, ctx->symq));
-  // Lambda (SRC/parquet_util.f90:311-314): constant per channel in the PA
+  // Lambda (SRC/parquet_util.f90:311-346): constant per channel in the PA,
+  // frequency-dependent tables from the two input files with DGA
   const double U = ctx->p.U;
   const double lam[4] = {U, -U, 2.0 * U, 0.0};
   size_t nL = (size_t)Nf * Nf * (Nf / 2);
-  for (int r = 0; r < 4; r++) {
-    std::vector<cplx> v(nL, make_double2(lam[r], 0.0));
-    TRY(upload(ctx, &t.L[r], v));
+  std::vector<cplx> Lr[4];
+  if (ctx->p.DGA) {
+    const std::string base = trim_name(ctx->p.fname_L);
+    TRY(read_lambda_file(ctx, base + "_ph.init", Nf, Lr[0], Lr[1]));
+    TRY(read_lambda_file(ctx, base + "_pp.init", Nf, Lr[2], Lr[3]));
+  } else {
+    for (int r = 0; r < 4; r++) Lr[r].assign(nL, make_double2(lam[r], 0.0));
   }
+  for (int r = 0; r < 4; r++) TRY(upload(ctx, &t.L[r], Lr[r]));
   // twiddles: e^{i*(-pi/beta*(2(nu-Nf/2)-1))*tau} (SRC/parquet_chi.f90:161)
   {
     std::vector<cplx> tw((size_t)Nf * Nf);
@@ -617,19 +667,17 @@ static int alloc_state(tups_ctx* ctx) {
   return TUPS_OK;
 }
 
-// vertex initialisation (SRC/preprocessing.f90:100-116): F = G = Lambda*Nc on
-// the (l=1, l=1) nu-block of every bosonic slot; Sigma = 0 or the DMFT input
+// vertex initialisation (SRC/preprocessing.f90:100-116): F = G = Lambda(:, :, w)*Nc
+// on the (l=1, l=1) nu-block of every bosonic slot; Sigma = 0 or the DMFT input
 static int init_state(tups_ctx* ctx) {
   const tups_dims& d = ctx->d;
   auto& s = ctx->s;
   const size_t Nz = d.Nz, Nb = d.Nb;
-  const double U = ctx->p.U;
-  const double lam[4] = {U, -U, 2.0 * U, 0.0};
   for (int r = 0; r < 4; r++) {
     const size_t bytes = Nz * Nz * Nb * sizeof(cplx);
     TRY(tups::cuda_check(ctx, cudaMemsetAsync(s.F[r], 0, bytes, ctx->stream), "init F"));
     TRY(tups::cuda_check(ctx, cudaMemsetAsync(s.G[r], 0, bytes, ctx->stream), "init G"));
-    TRY(tups::launch_fill_lambda_block(ctx, s.F[r], s.G[r], lam[r] * ctx->aux));
+    TRY(tups::launch_fill_lambda_block(ctx, s.F[r], s.G[r], ctx->t.L[r], ctx->aux));
   }
   TRY(tups::cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "init vertices"));
   std::vector<cplx> sig((size_t)d.Nt, make_double2(0.0, 0.0));

@@ -235,7 +235,7 @@ int launch_vertex_update(tups_ctx* ctx);
 int launch_output_mu(tups_ctx* ctx);
 int launch_fft2d(tups_ctx* ctx, const cplx* in, cplx* out, int forward);
 int launch_chi_aux(tups_ctx* ctx);
-int launch_fill_lambda_block(tups_ctx* ctx, cplx* F, cplx* G, double value);
+int launch_fill_lambda_block(tups_ctx* ctx, cplx* F, cplx* G, const cplx* L, double aux);
 int launch_grt_pre(tups_ctx* ctx, cplx* out);
 int launch_fft2d_batch(tups_ctx* ctx, const cplx* in, cplx* out, int nslices, int forward);
 int launch_readout(tups_ctx* ctx);
