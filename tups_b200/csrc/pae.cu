@@ -112,7 +112,7 @@ __device__ __forceinline__ void dmma_16x8x8(double* c, const double* a, const do
 }
 
 #ifndef PAE_MIN_BLOCKS
-#define PAE_MIN_BLOCKS 3  // CTAs per SM asked of ptxas for the 8-warp, <= 2 n-tile configs
+#define PAE_MIN_BLOCKS 3  // CTAs per SM asked of ptxas for the 8-warp, <= 2 n-tile configs (2 beyond)
 #endif
 constexpr int PAE_BK = 16;
 constexpr int PAE_LDB = PAE_BK + 4;
@@ -142,24 +142,33 @@ __global__ void k_pae_base(PaePtrs P, const int* __restrict__ ibz, int Nz, int N
   }
 }
 
-// One CTA per (tile of 32 listed elements, target pair x column chunk, q) for
-// one family: C^T[(target, element), (l1,l2)] = X^T[(target, element), (l3,l4,R)] M^T
-// and F_target += C / Nx.  Warps: 4 along rows (16 rows each) x WN along
+// One CTA per (tile of E = 8 RW listed elements, target pair x column chunk, q)
+// for one family: C^T[(target, element), (l1,l2)] = X^T[(target, element), (l3,l4,R)] M^T
+// and F_target += C / Nx.  Warps: RW along rows (16 rows each) x WN along
 // the (l1,l2) columns, TN n8 tiles each; BN = 8 TN WN >= Nl^2 (or a chunk).
-template <int TN, int WN, int RW>
-__global__ void __launch_bounds__(32 * RW * WN, RW * WN == 8 && TN <= 2 ? PAE_MIN_BLOCKS : 1)
+// The X operand is copied raw: cp.async brings the Phi(R) entries of the two
+// source channels for the K step STG-1 ahead into shared memory, and the
+// dispatch factors, the time-reversal conjugation and its form-factor sign
+// are applied when the MMA fragments are read, so no warp waits on a gather
+// between K steps.  The per-k offsets into Phi(R) and the signs s(l3) s(l4)
+// are tabulated once per CTA.
+template <int TN, int WN, int RW, int STG>
+__global__ void __launch_bounds__(32 * RW * WN, RW * WN == 8 ? (TN <= 2 ? PAE_MIN_BLOCKS : 2) : 1)
     k_pae_mma(PaePtrs P, const int4* __restrict__ elems, const int* __restrict__ counts,
               const int* __restrict__ ibz, const int* __restrict__ signs, int Nz, int Nf, int Nl, int NIBZ, int NR,
-              int nchunks, int fam, double inv_nx) {
+              int nchunks, int fam, int Kpad, double inv_nx) {
   constexpr int BN = 8 * TN * WN;
   constexpr int NT = 32 * RW * WN;
-  constexpr int PAE_E = 8 * RW;           // listed elements per CTA
-  constexpr int PAE_LDA = 2 * PAE_E + 2;  // (target, element) rows + pad
+  constexpr int E = 8 * RW;      // listed elements per CTA
+  constexpr int LDX = E + 2;     // elements + pad
+  static_assert(E % 16 == 0, "a warp's 16 rows must share one target");
   extern __shared__ __align__(16) unsigned char smraw[];
-  cplx* sA = reinterpret_cast<cplx*>(smraw);      // [2][BK][LDA]
-  cplx* sB = sA + 2 * PAE_BK * PAE_LDA;           // [2][BN][LDB]
-  __shared__ int e_w2[PAE_E], e_a[PAE_E], e_b[PAE_E], e_tr[PAE_E], e_nu1[PAE_E], e_nu2[PAE_E];
-  __shared__ double s_sg[16];
+  cplx* sX = reinterpret_cast<cplx*>(smraw);                                  // [STG][2][BK][LDX]
+  cplx* sB = sX + (size_t)STG * 2 * PAE_BK * LDX;                             // [STG][BN][LDB]
+  long long* koff = reinterpret_cast<long long*>(sB + (size_t)STG * BN * PAE_LDB);  // [Kpad]
+  double* ksg = reinterpret_cast<double*>(koff + Kpad);                       // [Kpad]
+  __shared__ long long e_off[E];
+  __shared__ int e_ok[E], e_tr[E], e_nu1[E], e_nu2[E];
   __shared__ double fac[2][2];
   __shared__ int src0;
 
@@ -174,24 +183,37 @@ __global__ void __launch_bounds__(32 * RW * WN, RW * WN == 8 && TN <= 2 ? PAE_MI
   const int nh = Nf / 2;
   const int list = pae_list(pair, fam, W, nh);
   const int cnt = counts[list];
-  const int e0 = tile * PAE_E;
+  const int e0 = tile * E;
   if (e0 >= cnt) return;
   const int nl2 = Nl * Nl, nl4 = nl2 * nl2;
   const int K = nl2 * NR;
   const size_t n2 = (size_t)Nz * Nz;
   const int tid = threadIdx.x;
 
-  if (tid < PAE_E) {
+  if (tid < E) {
     int4 rec = make_int4(0, 0, 1, 1);
     if (e0 + tid < cnt) rec = elems[(size_t)list * Nf * Nf + e0 + tid];
+    const int w2 = rec.y, a = rec.z, b = rec.w & 65535;
     e_nu1[tid] = rec.x & 255;
     e_nu2[tid] = rec.x >> 8;
-    e_w2[tid] = rec.y;
-    e_a[tid] = rec.z;
-    e_b[tid] = rec.w & 65535;
+    e_ok[tid] = w2 != 0;
     e_tr[tid] = rec.w >> 16;
+    // element part of the Phi(R) index (a-1) + Nz (b-1) + Nz^2 (w2-1)
+    e_off[tid] = w2 != 0 ? (long long)(a - 1) + (long long)Nz * (b - 1) + (long long)n2 * (w2 - 1) : 0;
   }
-  if (tid < Nl) s_sg[tid] = (double)signs[tid];
+  // k part of the index l3 Nf + Nz l4 Nf + Nz^2 (Nf/2) R, and s(l3) s(l4)
+  for (int k = tid; k < Kpad; k += NT) {
+    long long off = 0;
+    double sg = 1.0;
+    if (k < K) {
+      const int l34 = k % nl2, R = k / nl2;
+      const int l3 = l34 % Nl, l4 = l34 / Nl;
+      off = (long long)l3 * Nf + (long long)Nz * l4 * Nf + (long long)n2 * nh * R;
+      sg = (double)(signs[l3] * signs[l4]);
+    }
+    koff[k] = off;
+    ksg[k] = sg;
+  }
   if (tid == 0) {
     // dispatch factors fac[source][target] of this family (SRC/parquet_EQOuter.f90:84-113)
     // pair 0: D = phbar_to_ph from (d, m), A = pp_to_ph from (s, t)
@@ -205,46 +227,20 @@ __global__ void __launch_bounds__(32 * RW * WN, RW * WN == 8 && TN <= 2 ? PAE_MI
   const cplx* Mf = P.M[pair == 0 ? (fam == 0 ? 0 : 1) : (fam == 0 ? 3 : 2)];
   __syncthreads();
 
-  // gather of one K step into registers: thread -> (element, kk) pairs
-  constexpr int APER = PAE_E * PAE_BK / NT > 0 ? PAE_E * PAE_BK / NT : 1;
-  cplx ra[APER], rb[APER];
-  auto gather = [&](int kt) {
-#pragma unroll
-    for (int i = 0; i < APER; i++) {
-      const int p = tid + i * NT;
-      ra[i] = rb[i] = cmk(0.0, 0.0);
-      if (p >= PAE_E * PAE_BK) continue;
-      const int e = p % PAE_E, kk = p / PAE_E;
+  const cplx* X0 = P.PhiR[src0];
+  const cplx* X1 = P.PhiR[src0 + 1];
+  // one K step: raw X (2 sources x BK x E) and M^T (BN x BK), zero-filled
+  // outside K, past the list and for columns beyond Nl^2
+  auto load_stage = [&](int stage, int kt) {
+    cplx* dX = sX + (size_t)stage * 2 * PAE_BK * LDX;
+    for (int p = tid; p < 2 * E * PAE_BK; p += NT) {
+      const int e = p % E, rest = p / E;
+      const int kk = rest % PAE_BK, src = rest / PAE_BK;
       const int k = kt * PAE_BK + kk;
-      if (k >= K) continue;
-      const int w2 = e_w2[e];
-      if (w2 == 0) continue;
-      const int l34 = k % nl2, R = k / nl2;
-      const int l3 = l34 % Nl, l4 = l34 / Nl;
-      const size_t xi = (size_t)(l3 * Nf + e_a[e] - 1) + (size_t)Nz * (l4 * Nf + e_b[e] - 1) +
-                        n2 * ((size_t)(w2 - 1) + (size_t)nh * R);
-      cplx x0 = __ldg(P.PhiR[src0] + xi), x1 = __ldg(P.PhiR[src0 + 1] + xi);
-      if (e_tr[e]) {
-        const double sg = s_sg[l3] * s_sg[l4];
-        x0 = cmk(sg * x0.x, -sg * x0.y);
-        x1 = cmk(sg * x1.x, -sg * x1.y);
-      }
-      ra[i] = cmk(fac[0][0] * x0.x + fac[1][0] * x1.x, fac[0][0] * x0.y + fac[1][0] * x1.y);
-      rb[i] = cmk(fac[0][1] * x0.x + fac[1][1] * x1.x, fac[0][1] * x0.y + fac[1][1] * x1.y);
+      const bool ok = k < K && e_ok[e];
+      const cplx* g = src ? X1 : X0;
+      cp_async16p(dX + (src * PAE_BK + kk) * LDX + e, ok ? g + e_off[e] + koff[k] : g, ok);
     }
-  };
-  auto store_a = [&](int stage) {
-    cplx* dA = sA + (size_t)stage * PAE_BK * PAE_LDA;
-#pragma unroll
-    for (int i = 0; i < APER; i++) {
-      const int p = tid + i * NT;
-      if (p >= PAE_E * PAE_BK) continue;
-      const int e = p % PAE_E, kk = p / PAE_E;
-      dA[kk * PAE_LDA + e] = ra[i];
-      dA[kk * PAE_LDA + PAE_E + e] = rb[i];
-    }
-  };
-  auto load_b = [&](int stage, int kt) {
     cplx* dB = sB + (size_t)stage * BN * PAE_LDB;
     for (int p = tid; p < BN * PAE_BK; p += NT) {
       const int kk = p % PAE_BK, n = p / PAE_BK;
@@ -264,36 +260,52 @@ __global__ void __launch_bounds__(32 * RW * WN, RW * WN == 8 && TN <= 2 ? PAE_MI
   const int lane = tid & 31, warp = tid >> 5;
   const int wr = warp % RW, wc = warp / RW;
   const int gid = lane >> 2, tig = lane & 3;
+  const int tgt = (wr * 16) / E;            // the warp's target channel
+  const int er = (wr * 16) % E + gid;       // its elements er and er + 8
+  const double fa = fac[0][tgt], fb = fac[1][tgt];
+  const bool tr0 = e_tr[er] != 0, tr1 = e_tr[er + 8] != 0;
   double cre[TN][4], cim[TN][4];
 #pragma unroll
   for (int j = 0; j < TN; j++)
 #pragma unroll
     for (int x = 0; x < 4; x++) cre[j][x] = cim[j][x] = 0.0;
 
-  const int kt_hi = (K + PAE_BK - 1) / PAE_BK;
-  gather(0);
-  load_b(0, 0);
-  store_a(0);
-  for (int kt = 0; kt < kt_hi; kt++) {
-    const int cur = kt & 1;
-    asm volatile("cp.async.wait_group 0;\n" ::);
-    __syncthreads();
-    if (kt + 1 < kt_hi) {
-      gather(kt + 1);
-      load_b(cur ^ 1, kt + 1);
+  // fragment value of element e at k: fa x0 + fb x1, conjugated with sign
+  // s(l3) s(l4) for time-reversed elements
+  auto xval = [&](const cplx* cX, int kk, int e, bool trv, double sg, double& re, double& im) {
+    const cplx x0 = cX[kk * LDX + e], x1 = cX[(PAE_BK + kk) * LDX + e];
+    re = fa * x0.x + fb * x1.x;
+    im = fa * x0.y + fb * x1.y;
+    if (trv) {
+      re = sg * re;
+      im = -sg * im;
     }
-    const cplx* cA = sA + (size_t)cur * PAE_BK * PAE_LDA;
-    const cplx* cB = sB + (size_t)cur * BN * PAE_LDB;
+  };
+
+  const int kt_hi = Kpad / PAE_BK;
+#pragma unroll
+  for (int st = 0; st < STG - 1; st++) {
+    if (st < kt_hi) load_stage(st, st);
+    else asm volatile("cp.async.commit_group;\n" ::);
+  }
+  for (int kt = 0; kt < kt_hi; kt++) {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(STG - 2));
+    __syncthreads();
+    {
+      const int nk = kt + STG - 1;
+      if (nk < kt_hi) load_stage(nk % STG, nk);
+      else asm volatile("cp.async.commit_group;\n" ::);
+    }
+    const cplx* cX = sX + (size_t)(kt % STG) * 2 * PAE_BK * LDX;
+    const cplx* cB = sB + (size_t)(kt % STG) * BN * PAE_LDB;
 #pragma unroll
     for (int k8 = 0; k8 < PAE_BK; k8 += 8) {
       double are[4], aim[4], anim[4];
-      const int mb = wr * 16 + gid;
-      const cplx v0 = cA[(k8 + tig) * PAE_LDA + mb], v1 = cA[(k8 + tig) * PAE_LDA + mb + 8];
-      const cplx v2 = cA[(k8 + tig + 4) * PAE_LDA + mb], v3 = cA[(k8 + tig + 4) * PAE_LDA + mb + 8];
-      are[0] = v0.x; aim[0] = v0.y;
-      are[1] = v1.x; aim[1] = v1.y;
-      are[2] = v2.x; aim[2] = v2.y;
-      are[3] = v3.x; aim[3] = v3.y;
+      const double sa = ksg[kt * PAE_BK + k8 + tig], sb = ksg[kt * PAE_BK + k8 + tig + 4];
+      xval(cX, k8 + tig, er, tr0, sa, are[0], aim[0]);
+      xval(cX, k8 + tig, er + 8, tr1, sa, are[1], aim[1]);
+      xval(cX, k8 + tig + 4, er, tr0, sb, are[2], aim[2]);
+      xval(cX, k8 + tig + 4, er + 8, tr1, sb, are[3], aim[3]);
 #pragma unroll
       for (int x = 0; x < 4; x++) anim[x] = -aim[x];
 #pragma unroll
@@ -307,8 +319,8 @@ __global__ void __launch_bounds__(32 * RW * WN, RW * WN == 8 && TN <= 2 ? PAE_MI
         dmma_16x8x8(cim[j], aim, bre);
       }
     }
-    if (kt + 1 < kt_hi) store_a(cur ^ 1);
   }
+  asm volatile("cp.async.wait_group 0;\n" ::);
 
   // epilogue: F_target += C / Nx on the listed elements (each element is in
   // a family's list once, so a pass writes it at most once)
@@ -316,9 +328,8 @@ __global__ void __launch_bounds__(32 * RW * WN, RW * WN == 8 && TN <= 2 ? PAE_MI
   for (int j = 0; j < TN; j++)
 #pragma unroll
     for (int x = 0; x < 4; x++) {
-      const int row = wr * 16 + gid + (x >= 2 ? 8 : 0);
+      const int e = er + (x >= 2 ? 8 : 0);
       const int col = chunk * BN + (wc * TN + j) * 8 + 2 * tig + (x & 1);
-      const int tgt = row / PAE_E, e = row % PAE_E;
       if (col >= nl2 || e0 + e >= cnt) continue;
       const int nu1 = e_nu1[e], nu2 = e_nu2[e];
       const int l1 = col % Nl, l2 = col / Nl;
@@ -329,14 +340,17 @@ __global__ void __launch_bounds__(32 * RW * WN, RW * WN == 8 && TN <= 2 ? PAE_MI
     }
 }
 
-template <int TN, int WN, int RW>
+template <int TN, int WN, int RW, int STG>
 static int run_pae(tups_ctx* ctx, const PaePtrs& P, int nchunks, int fam, int max_count) {
   const auto& d = ctx->d;
   constexpr int BN = 8 * TN * WN;
   constexpr int E = 8 * RW;
-  constexpr int LDA = 2 * E + 2;
-  const size_t sm = (size_t)(2 * PAE_BK * LDA + 2 * BN * PAE_LDB) * sizeof(cplx);
-  auto kern = k_pae_mma<TN, WN, RW>;
+  constexpr int LDX = E + 2;
+  const int K = d.Nl * d.Nl * d.NR;
+  const int Kpad = (K + PAE_BK - 1) / PAE_BK * PAE_BK;
+  const size_t sm = (size_t)(STG * 2 * PAE_BK * LDX + STG * BN * PAE_LDB) * sizeof(cplx) +
+                    (size_t)Kpad * (sizeof(long long) + sizeof(double));
+  auto kern = k_pae_mma<TN, WN, RW, STG>;
   if (sm > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return cuda_check(ctx, e, "k_pae_mma smem attribute");
@@ -345,7 +359,7 @@ static int run_pae(tups_ctx* ctx, const PaePtrs& P, int nchunks, int fam, int ma
   if (max_tiles == 0) return TUPS_OK;
   dim3 grid(d.NIBZ, max_tiles * 2 * nchunks, d.Nf / 2);
   kern<<<grid, 32 * RW * WN, sm, ctx->stream>>>(P, ctx->t.pae_elems, ctx->t.pae_counts, ctx->t.ibz, ctx->t.signs,
-                                                d.Nz, d.Nf, d.Nl, d.NIBZ, d.NR, nchunks, fam, 1.0 / d.Nx);
+                                                d.Nz, d.Nf, d.Nl, d.NIBZ, d.NR, nchunks, fam, Kpad, 1.0 / d.Nx);
   return after_launch(ctx, "k_pae_mma");
 }
 
@@ -415,11 +429,12 @@ int launch_pae(tups_ctx* ctx) {
   for (int fam = 0; fam < 2; fam++) {
     const int mc = ctx->pae_max_tiles[fam];
     // tile configs measured on a B200: 8 warps x 32 elements at Nl^2 <= 32
-    // (8x8 / Nl = 5: 2.0 ms against 2.7 ms with 64 elements), 16 warps x 64
-    // elements beyond (16x16 / Nl = 9: 598 ms against 753 ms with 32)
-    if (nl2 <= 8) rc = run_pae<1, 1, 4>(ctx, P, 1, fam, mc);
-    else if (nl2 <= 32) rc = run_pae<2, 2, 4>(ctx, P, 1, fam, mc);
-    else rc = run_pae<6, 2, 8>(ctx, P, (nl2 + 95) / 96, fam, mc);
+    // (8x8 / Nl = 5: 1.83 ms), 8 warps x 32 elements x 96 columns with two
+    // CTAs per SM beyond (16x16 / Nl = 9: 482 ms; one 16-warp CTA of 64
+    // elements per SM 540 ms, 64 elements x 48 columns in two chunks 491 ms)
+    if (nl2 <= 8) rc = run_pae<1, 1, 4, 2>(ctx, P, 1, fam, mc);
+    else if (nl2 <= 32) rc = run_pae<2, 2, 4, 2>(ctx, P, 1, fam, mc);
+    else rc = run_pae<6, 2, 4, 2>(ctx, P, (nl2 + 95) / 96, fam, mc);
     if (rc) return rc;
   }
   return TUPS_OK;
