@@ -418,7 +418,10 @@ int launch_bse_chunk(tups_ctx* ctx, int q_begin, int q_count) {
   // three real products at Nz = 160 (1.93 ms against 2.13 ms with four;
   // 2.4-2.8 ms with 4 stages, BK = 32 or 2 warps)
   if (d.Nz % 64 == 0 || d.Nz > 512) rc = run_gemm<64, 64, 16, 2, 4, 3, false>(ctx, P, q_begin, q_count);
-  else if (d.Nz >= 32) rc = run_gemm<32, 32, 16, 2, 2, 3, true>(ctx, P, q_begin, q_count);
+  // 32 x 32 tiles: two stages (38 KB of shared memory, 5 CTAs per SM by
+  // registers) measured 1.79 ms at 8x8 / Nl = 5 against 1.93 ms with three
+  // stages (57 KB, 4 CTAs per SM) and 2.01 ms with two stages of BK = 32
+  else if (d.Nz >= 32) rc = run_gemm<32, 32, 16, 2, 2, 2, true>(ctx, P, q_begin, q_count);
   else rc = run_gemm<16, 16, 16, 1, 2, 3, true>(ctx, P, q_begin, q_count);
   phase_end(ctx, TUPS_PHASE_BSE_GEMM);
   return rc;
