@@ -35,6 +35,7 @@ extern "C" {
 #define TUPS_ERR_BADARG (-7)    /* bad argument (NULL pointer, index range) */
 #define TUPS_ERR_IO (-8)        /* input file unreadable or malformed */
 #define TUPS_ERR_STATE (-9)     /* call order violated (e.g. PAE before PhiR) */
+#define TUPS_ERR_COMM (-10)     /* a host exchange between ranks failed */
 
 /* channel numbering as in the reference's select case(channel): d, m, s, t */
 #define TUPS_CH_D 0
@@ -104,6 +105,38 @@ int tups_read_prms(const char* path, tups_params* out);
  * fills device state on `device`. */
 int tups_ctx_create(const tups_params* p, int device, tups_ctx** out);
 int tups_ctx_destroy(tups_ctx* ctx);
+
+/* Slot-sharded context: rank `rank` of `ntasks` holds the contiguous bosonic
+ * slots [rank*Nb, (rank+1)*Nb), Nb = Nred/ntasks, as the reference's MPI ranks
+ * do (`Nb = Nred/ntasks`, `id*Nb + idx_q`: SRC/parquet_ini.f90:346-349,
+ * SRC/preprocessing.f90:98-116); ntasks must divide Nred, as the reference
+ * requires (SRC/preprocessing.f90:94-97).  Vertices, chi and the BSE are
+ * local; Phi(R), Sigma and mu are replicated.  The three steps that need
+ * every slot call the exchange function set by tups_set_exchange: the
+ * Phi(R) partial sums over the rank's momenta (communicatePhis /
+ * FTPhis, SRC/parquet_PhiR.f90:114-258), the self-energy sum over slots
+ * (SRC/parquet_SDE.f90:221-258) and max|F_r| of conv
+ * (SRC/parquet_check.f90:109-117).  Iterations of a sharded context are not
+ * replayed from CUDA graphs, and tups_readout needs an unsharded context. */
+int tups_ctx_create_sharded(const tups_params* p, int device, int rank, int ntasks, tups_ctx** out);
+
+/* Exchange between the ranks of a sharded context: combine `count` doubles
+ * at device address `data` over all ranks, in place (op TUPS_XCH_SUM or
+ * TUPS_XCH_MAX), and return 0, or nonzero on failure (the library then
+ * returns TUPS_ERR_COMM).  `what` names the buffer: TUPS_XCH_PHIR + r for
+ * Phi(R) of channel r (0..3), TUPS_XCH_SIGMAV, TUPS_XCH_FMAX.  The library
+ * synchronises its stream before the call; the data must be complete in
+ * device memory when the function returns.  Every rank makes the same calls
+ * in the same order. */
+typedef int (*tups_exchange_fn)(void* user, int what, double* data, size_t count, int op);
+#define TUPS_XCH_SUM 0
+#define TUPS_XCH_MAX 1
+#define TUPS_XCH_PHIR 0
+#define TUPS_XCH_SIGMAV 4
+#define TUPS_XCH_FMAX 5
+int tups_set_exchange(tups_ctx* ctx, tups_exchange_fn fn, void* user);
+/* rank, ntasks and the first global slot of this context (0, 1, 0 unsharded) */
+int tups_get_shard(const tups_ctx* ctx, int* rank, int* ntasks, int* slot0);
 /* Host-only part of tups_ctx_create (no device needed): derived sizes and the
  * form-factor / symmetry / index tables in the layouts of tups_get_tables.
  * Lets a caller size its host arrays before creating a context. Any output

@@ -51,10 +51,17 @@ class tups_conv_info(C.Structure):
                 ("bisection_steps", C.c_int), ("converged", C.c_int)]
 
 
+# int (*)(void* user, int what, double* data, size_t count, int op): the host
+# exchange of a sharded context (tups_set_exchange)
+EXCHANGE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_size_t, C.c_int)
+
 # (name, argtypes); every function returns int unless listed in _SPECIAL
 _PROTOS = {
     "tups_read_prms": [C.c_char_p, C.POINTER(tups_params)],
     "tups_ctx_create": [C.POINTER(tups_params), C.c_int, C.POINTER(C.c_void_p)],
+    "tups_ctx_create_sharded": [C.POINTER(tups_params), C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p)],
+    "tups_set_exchange": [C.c_void_p, C.c_void_p, C.c_void_p],
+    "tups_get_shard": [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)],
     "tups_ctx_destroy": [C.c_void_p],
     "tups_host_tables": [C.POINTER(tups_params), C.POINTER(tups_dims)] + [C.c_void_p] * 7,
     "tups_get_dims": [C.c_void_p, C.POINTER(tups_dims)],

@@ -318,6 +318,7 @@ static int readout_async(tups_ctx* ctx) {
 extern "C" int tups_readout(tups_ctx* ctx, int ite) {
   (void)ite;
   if (!ctx) return TUPS_ERR_BADARG;
+  if (ctx->ntasks > 1) return tups::set_error(ctx, TUPS_ERR_STATE, "the readout needs every slot: use an unsharded context");
   TRY(set_dev(ctx));
   TRY(readout_async(ctx));
   TRY(device_status(ctx));
@@ -348,7 +349,9 @@ static int iteration_impl(tups_ctx* ctx, int ite, tups_conv_info* info, bool wit
 static int iteration_graph(tups_ctx* ctx, int ite, tups_conv_info* info);
 
 extern "C" int tups_iteration(tups_ctx* ctx, int ite, tups_conv_info* info) {
-  if (ctx && ctx->use_graph && ite > 0 && ctx->have_exp && ctx->have_M && !ctx->timing)
+  // a sharded context calls the host exchange inside the iteration, which a
+  // graph cannot hold
+  if (ctx && ctx->use_graph && ite > 0 && ctx->have_exp && ctx->have_M && !ctx->timing && ctx->ntasks == 1)
     return iteration_graph(ctx, ite, info);
   return iteration_impl(ctx, ite, info, false);
 }
@@ -456,7 +459,7 @@ static int iteration_impl(tups_ctx* ctx, int ite, tups_conv_info* info, bool wit
   if (info) *info = ci;
   if (rc) return rc;
   if (ite % 5 == 0 || ite == ctx->p.ite_max - 1 || ci.converged) {
-    if (with_readout) TRY(readout_async(ctx));
+    if (with_readout && ctx->ntasks == 1) TRY(readout_async(ctx));
     else TRY(tups::launch_output_mu(ctx));
   }
   tups::phase_begin(ctx, TUPS_PHASE_UPDATE);

@@ -113,7 +113,7 @@ int launch_chi(tups_ctx* ctx, int q_begin, int q_count) {
   const auto& d = ctx->d;
   dim3 grid(q_count, d.Nf);
   size_t sm = 2 * (size_t)d.Nc * sizeof(cplx);
-  k_chi_blocks<<<grid, 128, sm, ctx->stream>>>(ctx->s.Sigma, ctx->s.SigmaH, ctx->t.Ekg, ctx->t.FF, ctx->t.ibz,
+  k_chi_blocks<<<grid, 128, sm, ctx->stream>>>(ctx->s.Sigma, ctx->s.SigmaH, ctx->t.Ekg, ctx->t.FF, ibz_local(ctx),
                                                ctx->s.scal, ctx->s.chi_ph, ctx->s.chi_pp, q_begin, d.Nx, d.Ny, d.Nf,
                                                d.Ngrain, d.Nl, ctx->p.beta);
   return after_launch(ctx, "k_chi_blocks");
@@ -123,7 +123,7 @@ int launch_chi_aux(tups_ctx* ctx) {
   const auto& d = ctx->d;
   dim3 grid(d.Nb, d.nbox);
   size_t sm = 2 * (size_t)d.Nc * sizeof(cplx);
-  k_chi_aux<<<grid, 128, sm, ctx->stream>>>(ctx->s.Sigma, ctx->s.SigmaH, ctx->t.Ekg, ctx->t.FF, ctx->t.ibz,
+  k_chi_aux<<<grid, 128, sm, ctx->stream>>>(ctx->s.Sigma, ctx->s.SigmaH, ctx->t.Ekg, ctx->t.FF, ibz_local(ctx),
                                             ctx->s.scal, ctx->s.chi_aux_ph, ctx->s.chi_aux_pp, d.Nx, d.Ny, d.Nf,
                                             d.Ngrain, d.Nl, ctx->p.f_range, ctx->p.beta);
   return after_launch(ctx, "k_chi_aux");

@@ -101,7 +101,7 @@ int launch_fill_lambda_block(tups_ctx* ctx, cplx* F, cplx* G, const cplx* L, dou
   const auto& d = ctx->d;
   const size_t n = (size_t)d.Nf * d.Nf * d.Nb;
   k_fill_lambda_block<<<(unsigned)std::min<size_t>(cdiv(n, 256), 148 * 8), 256, 0, ctx->stream>>>(
-      F, G, L, ctx->t.ibz, d.Nz, d.Nf, d.Nb, aux);
+      F, G, L, ibz_local(ctx), d.Nz, d.Nf, d.Nb, aux);
   return after_launch(ctx, "k_fill_lambda_block");
 }
 
@@ -130,7 +130,11 @@ int launch_conv(tups_ctx* ctx) {
   const size_t n = (size_t)d.Nz * d.Nz * d.Nb;
   dim3 grid((unsigned)std::min<size_t>(cdiv(n, 256), 148 * 8), 4);
   k_fmax<<<grid, 256, 0, ctx->stream>>>(ctx->s.F[0], ctx->s.F[1], ctx->s.F[2], ctx->s.F[3], n, ctx->s.scal);
-  return after_launch(ctx, "k_fmax");
+  rc = after_launch(ctx, "k_fmax");
+  if (rc) return rc;
+  // max|F_r| (4 values) and the NaN flag over the ranks of a sharded context
+  static_assert(S_NANFLAG == S_FMAX + 4, "exchanged as one range");
+  return exchange(ctx, TUPS_XCH_FMAX, ctx->s.scal + S_FMAX, 5, TUPS_XCH_MAX);
 }
 
 int launch_vertex_update(tups_ctx* ctx) {

@@ -159,7 +159,7 @@ template <int TN, int WN, int RW, int STG>
 __global__ void __launch_bounds__(32 * RW * WN, RW * WN == 8 ? (TN <= 2 ? PAE_MIN_BLOCKS : 2) : 1)
     k_pae_mma(PaePtrs P, const int4* __restrict__ elems, const int* __restrict__ counts,
               const int* __restrict__ ibz, const int* __restrict__ signs, int Nz, int Nf, int Nl, int NIBZ, int NR,
-              int nchunks, int fam, int Kpad, double inv_nx) {
+              int nchunks, int fam, int Kpad, int slot0, int Nb, double inv_nx) {
   constexpr int BN = 8 * TN * WN;
   constexpr int NT = 32 * RW * WN;
   constexpr int E = 8 * RW;      // listed elements per CTA
@@ -180,9 +180,12 @@ __global__ void __launch_bounds__(32 * RW * WN, RW * WN == 8 ? (TN <= 2 ? PAE_MI
   // depend on Q) and L2 serves all but the first
   const int pc = blockIdx.y % (2 * nchunks), tile = blockIdx.y / (2 * nchunks);
   const int pair = pc / nchunks, chunk = pc % nchunks;
-  const int q = blockIdx.x * (Nf / 2) + blockIdx.z;
+  // blockIdx.x runs over the IBZ momenta that hold this context's slots
+  const int Qi = slot0 / (Nf / 2) + blockIdx.x;
+  const int q = Qi * (Nf / 2) + blockIdx.z;  // global slot
+  const int lq = q - slot0;                  // its local index
+  if (lq < 0 || lq >= Nb) return;
   const int W = ibz[3 * q + 2];
-  const int Qi = q / (Nf / 2);
   const int nh = Nf / 2;
   const int list = pae_list(pair, fam, W, nh);
   const int cnt = counts[list];
@@ -343,7 +346,7 @@ __global__ void __launch_bounds__(32 * RW * WN, RW * WN == 8 ? (TN <= 2 ? PAE_MI
       const int nu1 = e_nu1[e], nu2 = e_nu2[e];
       const int l1 = col % Nl, l2 = col / Nl;
       const int r = (pair == 0 ? 0 : 2) + tgt;
-      const size_t idx = (size_t)(l1 * Nf + nu1 - 1) + (size_t)Nz * (l2 * Nf + nu2 - 1) + n2 * q;
+      const size_t idx = (size_t)(l1 * Nf + nu1 - 1) + (size_t)Nz * (l2 * Nf + nu2 - 1) + n2 * lq;
       const cplx f = P.F[r][idx];
       P.F[r][idx] = cmk(f.x + inv_nx * cre[j][x], f.y + inv_nx * cim[j][x]);
     }
@@ -366,9 +369,12 @@ static int run_pae(tups_ctx* ctx, const PaePtrs& P, int nchunks, int fam, int ma
   }
   const int max_tiles = (max_count + E - 1) / E;
   if (max_tiles == 0) return TUPS_OK;
-  dim3 grid(d.NIBZ, max_tiles * 2 * nchunks, d.Nf / 2);
+  const int nh = d.Nf / 2;
+  const int nQ = (ctx->slot0 + d.Nb - 1) / nh - ctx->slot0 / nh + 1;  // momenta holding this context's slots
+  dim3 grid(nQ, max_tiles * 2 * nchunks, nh);
   kern<<<grid, 32 * RW * WN, sm, ctx->stream>>>(P, ctx->t.pae_elems, ctx->t.pae_counts, ctx->t.ibz, ctx->t.signs,
-                                                d.Nz, d.Nf, d.Nl, d.NIBZ, d.NR, nchunks, fam, Kpad, 1.0 / d.Nx);
+                                                d.Nz, d.Nf, d.Nl, d.NIBZ, d.NR, nchunks, fam, Kpad, ctx->slot0,
+                                                d.Nb, 1.0 / d.Nx);
   return after_launch(ctx, "k_pae_mma");
 }
 
@@ -431,7 +437,7 @@ int launch_pae(tups_ctx* ctx) {
   // F = Phi + Lambda Nc, then the diagonal family, then the anti-diagonal one
   const size_t n = (size_t)d.Nz * d.Nz * d.Nb;
   dim3 bgrid((unsigned)std::min<size_t>(cdiv(n, 256), 148 * 8), 4);
-  k_pae_base<<<bgrid, 256, 0, ctx->stream>>>(P, ctx->t.ibz, d.Nz, d.Nf, d.Nb, std::fabs(1.0 / ctx->FF[0] * 1.0 / ctx->FF[0]));
+  k_pae_base<<<bgrid, 256, 0, ctx->stream>>>(P, ibz_local(ctx), d.Nz, d.Nf, d.Nb, std::fabs(1.0 / ctx->FF[0] * 1.0 / ctx->FF[0]));
   int rc = after_launch(ctx, "k_pae_base");
   if (rc) return rc;
   const int nl2 = d.Nl * d.Nl;

@@ -20,7 +20,7 @@ struct PhirPtrs {
 // Q carry expSqR = 0 and are skipped.
 __global__ void k_phir(PhirPtrs P, const cplx* __restrict__ expSqR, const int* __restrict__ symlist,
                        const int* __restrict__ lsym, const double* __restrict__ lfac, int Nz, int Nf, int Nl,
-                       int NIBZ, int NR, double inv_nx) {
+                       int NIBZ, int NR, int slot0, int Nb, double inv_nx) {
   // the phase tables (expSqR, star lists, l-space maps) of all threads in
   // shared memory: the inner loop reads only Phi from global memory
   extern __shared__ __align__(16) unsigned char phir_sm[];
@@ -46,14 +46,17 @@ __global__ void k_phir(PhirPtrs P, const cplx* __restrict__ expSqR, const int* _
   cplx acc[8];
 #pragma unroll
   for (int R = 0; R < 8; R++) acc[R] = cmk(0.0, 0.0);
-  const cplx* G = P.G[r] + n2 * (size_t)w;
+  const cplx* G = P.G[r];
   for (int s = 0; s < NS; s++) {
     const int lis = sL[s + NS * li], ljs = sL[s + NS * lj];
     const double f = sF[s + NS * li] * sF[s + NS * lj];
     const cplx* src = G + (size_t)(lis * Nf + ni) + (size_t)Nz * (ljs * Nf + nj);
     for (int Q = 0; Q < NIBZ; Q++) {
       if (!sSym[NS * Q + s]) continue;
-      const cplx v = cscale(__ldg(src + n2 * (size_t)Q * nh), f);
+      // slot (Q, w) is global slot Q nh + w; a sharded context sums its own
+      const int lq = Q * nh + w - slot0;
+      if (lq < 0 || lq >= Nb) continue;
+      const cplx v = cscale(__ldg(src + n2 * (size_t)lq), f);
       const cplx* eq = sE + Q + (size_t)NIBZ * NR * s;
 #pragma unroll
       for (int R = 0; R < 8; R++)
@@ -137,8 +140,14 @@ int launch_phir(tups_ctx* ctx) {
   }
   dim3 grid(cdiv(n2, 256), d.Nf / 2, 4);
   k_phir<<<grid, 256, sm, ctx->stream>>>(P, ctx->t.expSqR, ctx->t.symlist, ctx->t.lsym, ctx->t.lfac, d.Nz, d.Nf,
-                                         d.Nl, d.NIBZ, d.NR, 1.0 / d.Nx);
-  return after_launch(ctx, "k_phir");
+                                         d.Nl, d.NIBZ, d.NR, ctx->slot0, d.Nb, 1.0 / d.Nx);
+  int rc = after_launch(ctx, "k_phir");
+  if (rc) return rc;
+  // a sharded context summed over its own momenta: Phi(R) over all ranks
+  for (int r = 0; r < 4 && !rc; r++)
+    rc = exchange(ctx, TUPS_XCH_PHIR + r, reinterpret_cast<double*>(ctx->s.PhiR[r]),
+                  2 * n2 * (size_t)(d.Nf / 2) * d.NR, TUPS_XCH_SUM);
+  return rc;
 }
 
 int launch_M(tups_ctx* ctx, int which) {

@@ -102,7 +102,7 @@ __global__ void __launch_bounds__(256) k_sde_sigma(const cplx* __restrict__ Gkw,
                                                    const cplx* __restrict__ LChi, const cplx* __restrict__ PhChi,
                                                    const cplx* __restrict__ PPChi, const double* __restrict__ scal,
                                                    cplx* __restrict__ SigmaV, int Nx, int Ny, int Nf, int Nl, int Nz,
-                                                   int Nb, double beta, double pref) {
+                                                   int Nb, int slot0, double beta, double pref) {
   __shared__ double sh[32];
   const int ik = blockIdx.x, k0 = blockIdx.y + 1;
   const int nh = Nf / 2;
@@ -111,8 +111,9 @@ __global__ void __launch_bounds__(256) k_sde_sigma(const cplx* __restrict__ Gkw,
   const int mkx = (Nx - kx) % Nx, mky = (Ny - ky) % Ny;
   double sre = 0.0, sim = 0.0;
   for (int q = threadIdx.x; q < Nb; q += blockDim.x) {
-    const int w = ibz[3 * q + 2];
-    const int Qi = q / nh;
+    // local slot q of this context is global slot slot0 + q
+    const int w = ibz[3 * (slot0 + q) + 2];
+    const int Qi = (slot0 + q) / nh;
     const cplx* Lq = LChi + (size_t)Nz * q;
     const cplx* Pq = PhChi + (size_t)Nz * q;
     const cplx* Qq = PPChi + (size_t)Nz * q;
@@ -264,7 +265,7 @@ int launch_sde(tups_ctx* ctx) {
   }
   const double ff2 = 1.0 / (ctx->FF[0] * ctx->FF[0]);
   dim3 g1(cdiv(d.Nz, 32), d.Nb);
-  k_sde_chis<<<g1, dim3(32, 8), 0, ctx->stream>>>(P, ctx->s.chi_aux_ph, ctx->s.chi_aux_pp, ctx->t.ibz, ctx->s.LChi,
+  k_sde_chis<<<g1, dim3(32, 8), 0, ctx->stream>>>(P, ctx->s.chi_aux_ph, ctx->s.chi_aux_pp, ibz_local(ctx), ctx->s.LChi,
                                           ctx->s.PhChi, ctx->s.PPChi, d.Nz, d.Nf, d.Nl, ctx->p.f_range,
                                           ctx->p.use_U2, ctx->p.U, ff2);
   if ((rc = after_launch(ctx, "k_sde_chis"))) return rc;
@@ -273,8 +274,12 @@ int launch_sde(tups_ctx* ctx) {
   k_sde_sigma<<<g2, 256, 0, ctx->stream>>>(ctx->s.Gkw, ctx->s.SigmaH, ctx->t.Ek, ctx->t.FF_inv, ctx->t.signs,
                                            ctx->t.ibz, ctx->t.symlist, ctx->t.symq, ctx->s.LChi, ctx->s.PhChi,
                                            ctx->s.PPChi, ctx->s.scal, ctx->s.SigmaV, d.Nx, d.Ny, d.Nf, d.Nl, d.Nz,
-                                           d.Nb, ctx->p.beta, pref);
+                                           d.Nb, ctx->slot0, ctx->p.beta, pref);
   if ((rc = after_launch(ctx, "k_sde_sigma"))) return rc;
+  // a sharded context summed its own slots: Sigma_V over all ranks
+  if ((rc = exchange(ctx, TUPS_XCH_SIGMAV, reinterpret_cast<double*>(ctx->s.SigmaV), 2 * (size_t)d.NIBZ * d.Nf,
+                     TUPS_XCH_SUM)))
+    return rc;
   if (ctx->p.use_U2) {
     const int n1 = d.Nx * d.Ngrain, n2 = d.Ny * d.Ngrain;
     const size_t n = (size_t)n1 * n2 * d.Nf;

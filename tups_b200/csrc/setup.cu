@@ -21,6 +21,16 @@ int set_error(tups_ctx* ctx, int code, const std::string& msg) {
   return code;
 }
 
+int exchange(tups_ctx* ctx, int what, double* dev, size_t n, int op) {
+  if (ctx->ntasks <= 1) return TUPS_OK;
+  if (!ctx->xfn) return set_error(ctx, TUPS_ERR_STATE, "sharded context without an exchange function");
+  int rc = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "exchange");
+  if (rc) return rc;
+  if (ctx->xfn(ctx->xuser, what, dev, n, op) != 0)
+    return set_error(ctx, TUPS_ERR_COMM, "exchange " + std::to_string(what) + " between ranks failed");
+  return TUPS_OK;
+}
+
 int cuda_check(tups_ctx* ctx, cudaError_t e, const char* what) {
   if (e == cudaSuccess) return TUPS_OK;
   return set_error(ctx, e == cudaErrorMemoryAllocation ? TUPS_ERR_OOM : TUPS_ERR_CUDA,
@@ -726,13 +736,31 @@ static void free_all(tups_ctx* ctx) {
   ctx->stream = nullptr;
 }
 
-extern "C" int tups_ctx_create(const tups_params* p, int device, tups_ctx** out) {
+// Slots of rank `rank` of `ntasks` (SRC/parquet_ini.f90:346-349,
+// SRC/preprocessing.f90:94-116): Nb = Nred / ntasks contiguous slots from
+// rank * Nb; ntasks must divide Nred.
+static int shard_slots(tups_ctx* ctx, int rank, int ntasks) {
+  tups_dims& d = ctx->d;
+  if (ntasks < 1 || rank < 0 || rank >= ntasks)
+    return tups::set_error(ctx, TUPS_ERR_BADARG, "rank must lie in [0, ntasks)");
+  if (d.Nred % ntasks != 0)
+    return tups::set_error(ctx, TUPS_ERR_BADDIM, "choose the number of tasks such that it divides Nred = " +
+                                                    std::to_string(d.Nred));
+  d.Nb = d.Nred / ntasks;
+  ctx->rank = rank;
+  ctx->ntasks = ntasks;
+  ctx->slot0 = rank * d.Nb;
+  return TUPS_OK;
+}
+
+static int ctx_create(const tups_params* p, int device, int rank, int ntasks, tups_ctx** out) {
   if (!p || !out) return TUPS_ERR_BADARG;
   *out = nullptr;
   tups_ctx* ctx = new tups_ctx();
   ctx->p = *p;
   ctx->device = device;
   int rc = build_tables(ctx);
+  if (rc == TUPS_OK) rc = shard_slots(ctx, rank, ntasks);
   if (rc == TUPS_OK) rc = tups::cuda_check(ctx, cudaSetDevice(device), "cudaSetDevice");
   if (rc == TUPS_OK)
     rc = tups::cuda_check(ctx, cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking), "stream");
@@ -746,6 +774,29 @@ extern "C" int tups_ctx_create(const tups_params* p, int device, tups_ctx** out)
     return rc;
   }
   *out = ctx;
+  return TUPS_OK;
+}
+
+extern "C" int tups_ctx_create(const tups_params* p, int device, tups_ctx** out) {
+  return ctx_create(p, device, 0, 1, out);
+}
+
+extern "C" int tups_ctx_create_sharded(const tups_params* p, int device, int rank, int ntasks, tups_ctx** out) {
+  return ctx_create(p, device, rank, ntasks, out);
+}
+
+extern "C" int tups_set_exchange(tups_ctx* ctx, tups_exchange_fn fn, void* user) {
+  if (!ctx) return TUPS_ERR_BADARG;
+  ctx->xfn = fn;
+  ctx->xuser = user;
+  return TUPS_OK;
+}
+
+extern "C" int tups_get_shard(const tups_ctx* ctx, int* rank, int* ntasks, int* slot0) {
+  if (!ctx) return TUPS_ERR_BADARG;
+  if (rank) *rank = ctx->rank;
+  if (ntasks) *ntasks = ctx->ntasks;
+  if (slot0) *slot0 = ctx->slot0;
   return TUPS_OK;
 }
 
@@ -792,6 +843,7 @@ extern "C" const char* tups_strerror(int status) {
     case TUPS_ERR_BADARG: return "bad argument";
     case TUPS_ERR_IO: return "input file unreadable or malformed";
     case TUPS_ERR_STATE: return "call order violated";
+    case TUPS_ERR_COMM: return "exchange between ranks failed";
     default: return "unknown status";
   }
 }

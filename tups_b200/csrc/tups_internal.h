@@ -104,6 +104,10 @@ struct tups_ctx {
   tups_params p{};
   tups_dims d{};
   int device = 0;
+  // slot sharding: this context holds global slots [slot0, slot0 + d.Nb)
+  int rank = 0, ntasks = 1, slot0 = 0;
+  tups_exchange_fn xfn = nullptr;
+  void* xuser = nullptr;
   cudaStream_t stream = nullptr;
   std::string err;
   long long launches = 0;
@@ -211,6 +215,11 @@ void oz_bind_work(OzRun& R, const OzWork& w, void* base);
 int oz_run(OzRun& R, cudaStream_t stream, long long* launches);
 
 int set_error(tups_ctx* ctx, int code, const std::string& msg);
+// sharded contexts: combine n doubles at device address dev over the ranks
+// (no-op unsharded); synchronises the stream first
+int exchange(tups_ctx* ctx, int what, double* dev, size_t n, int op);
+// the ibz rows of this context's slots (local slot q -> global slot slot0 + q)
+inline const int* ibz_local(const tups_ctx* ctx) { return ctx->t.ibz + 3 * (size_t)ctx->slot0; }
 int cuda_check(tups_ctx* ctx, cudaError_t e, const char* what);
 // record a kernel launch and check for launch errors
 int after_launch(tups_ctx* ctx, const char* name);

@@ -137,15 +137,39 @@ def host_tables(params: Params) -> dict:
 class Solver:
     """One parquet solver instance with device-resident state."""
 
-    def __init__(self, params: Params, device: int = 0):
+    def __init__(self, params: Params, device: int = 0, rank: int = 0, ntasks: int = 1, exchange=None):
+        """``ntasks > 1``: this solver holds the bosonic slots of rank ``rank``
+        (``Nb = Nred / ntasks`` of them, from ``rank * Nb``), and ``exchange``
+        (a ``callable(what, device_ptr, count, op) -> None``, e.g.
+        ``tups_b200.sharded.TorchExchange``) combines the three buffers that
+        need every slot over the ranks."""
         self._lib = _lib.load()
         self.params = params
         self._cp = params.to_c()
         h = C.c_void_p()
-        rc = self._lib.tups_ctx_create(C.byref(self._cp), device, C.byref(h))
+        if ntasks > 1:
+            if exchange is None:
+                raise ValueError("a sharded solver needs an exchange function")
+            rc = self._lib.tups_ctx_create_sharded(C.byref(self._cp), device, rank, ntasks, C.byref(h))
+        else:
+            rc = self._lib.tups_ctx_create(C.byref(self._cp), device, C.byref(h))
         if rc != 0:
             raise TupsError(rc, "tups_ctx_create failed (see stderr)")
         self._ctx = h
+        self._xfn = None
+        if ntasks > 1:
+            def _xch(user, what, data, count, op):
+                try:
+                    exchange(int(what), int(data), int(count), int(op))
+                    return 0
+                except Exception as e:  # reported as TUPS_ERR_COMM by the library
+                    print(f"tups_b200 exchange {what} failed: {e!r}", flush=True)
+                    return 1
+            self._xfn = _lib.EXCHANGE_FN(_xch)  # kept alive with the solver
+            self._call("tups_set_exchange", C.cast(self._xfn, C.c_void_p), None)
+        r, n, s0 = C.c_int(), C.c_int(), C.c_int()
+        self._call("tups_get_shard", C.byref(r), C.byref(n), C.byref(s0))
+        self.rank, self.ntasks, self.slot0 = r.value, n.value, s0.value
         d = tups_dims()
         self._call("tups_get_dims", C.byref(d))
         self.dims = {f[0]: getattr(d, f[0]) for f in d._fields_}
