@@ -155,7 +155,7 @@ __global__ void k_pae_base(PaePtrs P, const int* __restrict__ ibz, int Nz, int N
 // are applied when the MMA fragments are read, so no warp waits on a gather
 // between K steps.  The per-k offsets into Phi(R) and the signs s(l3) s(l4)
 // are tabulated once per CTA.
-template <int TN, int WN, int RW, int STG>
+template <int TN, int WN, int RW, int STG, int QN>
 __global__ void __launch_bounds__(32 * RW * WN, RW * WN == 8 ? (TN <= 2 ? PAE_MIN_BLOCKS : 2) : 1)
     k_pae_mma(PaePtrs P, const int4* __restrict__ elems, const int* __restrict__ counts,
               const int* __restrict__ ibz, const int* __restrict__ signs, int Nz, int Nf, int Nl, int NIBZ, int NR,
@@ -180,13 +180,22 @@ __global__ void __launch_bounds__(32 * RW * WN, RW * WN == 8 ? (TN <= 2 ? PAE_MI
   // depend on Q) and L2 serves all but the first
   const int pc = blockIdx.y % (2 * nchunks), tile = blockIdx.y / (2 * nchunks);
   const int pair = pc / nchunks, chunk = pc % nchunks;
-  // blockIdx.x runs over the IBZ momenta that hold this context's slots
-  const int Qi = slot0 / (Nf / 2) + blockIdx.x;
-  const int q = Qi * (Nf / 2) + blockIdx.z;  // global slot
-  const int lq = q - slot0;                  // its local index
-  if (lq < 0 || lq >= Nb) return;
-  const int W = ibz[3 * q + 2];
+  // blockIdx.x runs over groups of QN IBZ momenta among those that hold this
+  // context's slots; the group's momenta sit side by side in the columns
+  // (momentum, (l1, l2)), so X serves all of them
   const int nh = Nf / 2;
+  const int w = blockIdx.z;
+  const int Qhi = (slot0 + Nb - 1) / nh;
+  const int Q0 = slot0 / nh + blockIdx.x * QN;
+  auto local_slot = [&](int iq) {  // local index of slot (Q0 + iq, w), or -1
+    const int lq = (Q0 + iq) * nh + w - slot0;
+    return (iq < QN && Q0 + iq <= Qhi && lq >= 0 && lq < Nb) ? lq : -1;
+  };
+  bool any = false;
+#pragma unroll
+  for (int iq = 0; iq < QN; iq++) any = any || local_slot(iq) >= 0;
+  if (!any) return;
+  const int W = ibz[3 * (Q0 * nh + w) + 2];  // the bosonic index of w, the same for every Q
   const int list = pae_list(pair, fam, W, nh);
   const int cnt = counts[list];
   const int e0 = tile * E;
@@ -251,12 +260,14 @@ __global__ void __launch_bounds__(32 * RW * WN, RW * WN == 8 ? (TN <= 2 ? PAE_MI
     for (int p = tid; p < BN * PAE_BK; p += NT) {
       const int kk = p % PAE_BK, n = p / PAE_BK;
       const int k = kt * PAE_BK + kk;
-      const int col = chunk * BN + n;
-      const bool ok = k < K && col < nl2;
+      const int nn = chunk * BN + n;
+      const int iq = QN == 1 ? 0 : nn / nl2;
+      const int col = nn - iq * nl2;
+      const bool ok = k < K && col < nl2 && iq < QN && Q0 + iq <= Qhi;
       const cplx* src = Mf;
       if (ok) {
         const int l34 = k % nl2, R = k / nl2;
-        src = Mf + col + (size_t)nl2 * l34 + (size_t)nl4 * (Qi + (size_t)NIBZ * R);
+        src = Mf + col + (size_t)nl2 * l34 + (size_t)nl4 * (Q0 + iq + (size_t)NIBZ * R);
       }
       cp_async16p(dB + n * PAE_LDB + kk, src, ok);
     }
@@ -341,8 +352,12 @@ __global__ void __launch_bounds__(32 * RW * WN, RW * WN == 8 ? (TN <= 2 ? PAE_MI
 #pragma unroll
     for (int x = 0; x < 4; x++) {
       const int e = er + (x >= 2 ? 8 : 0);
-      const int col = chunk * BN + (wc * TN + j) * 8 + 2 * tig + (x & 1);
+      const int nn = chunk * BN + (wc * TN + j) * 8 + 2 * tig + (x & 1);
+      const int iq = QN == 1 ? 0 : nn / nl2;
+      const int col = nn - iq * nl2;
       if (col >= nl2 || e0 + e >= cnt) continue;
+      const int lq = local_slot(iq);
+      if (lq < 0) continue;
       const int nu1 = e_nu1[e], nu2 = e_nu2[e];
       const int l1 = col % Nl, l2 = col / Nl;
       const int r = (pair == 0 ? 0 : 2) + tgt;
@@ -352,7 +367,7 @@ __global__ void __launch_bounds__(32 * RW * WN, RW * WN == 8 ? (TN <= 2 ? PAE_MI
     }
 }
 
-template <int TN, int WN, int RW, int STG>
+template <int TN, int WN, int RW, int STG, int QN = 1>
 static int run_pae(tups_ctx* ctx, const PaePtrs& P, int nchunks, int fam, int max_count) {
   const auto& d = ctx->d;
   constexpr int BN = 8 * TN * WN;
@@ -362,7 +377,7 @@ static int run_pae(tups_ctx* ctx, const PaePtrs& P, int nchunks, int fam, int ma
   const int Kpad = (K + PAE_BK - 1) / PAE_BK * PAE_BK;
   const size_t sm = (size_t)(STG * 2 * PAE_BK * LDX + STG * BN * PAE_LDB) * sizeof(cplx) +
                     (size_t)Kpad * (sizeof(long long) + sizeof(double));
-  auto kern = k_pae_mma<TN, WN, RW, STG>;
+  auto kern = k_pae_mma<TN, WN, RW, STG, QN>;
   if (sm > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return cuda_check(ctx, e, "k_pae_mma smem attribute");
@@ -371,7 +386,7 @@ static int run_pae(tups_ctx* ctx, const PaePtrs& P, int nchunks, int fam, int ma
   if (max_tiles == 0) return TUPS_OK;
   const int nh = d.Nf / 2;
   const int nQ = (ctx->slot0 + d.Nb - 1) / nh - ctx->slot0 / nh + 1;  // momenta holding this context's slots
-  dim3 grid(nQ, max_tiles * 2 * nchunks, nh);
+  dim3 grid((nQ + QN - 1) / QN, max_tiles * 2 * nchunks, nh);
   kern<<<grid, 32 * RW * WN, sm, ctx->stream>>>(P, ctx->t.pae_elems, ctx->t.pae_counts, ctx->t.ibz, ctx->t.signs,
                                                 d.Nz, d.Nf, d.Nl, d.NIBZ, d.NR, nchunks, fam, Kpad, ctx->slot0,
                                                 d.Nb, 1.0 / d.Nx);
@@ -443,11 +458,14 @@ int launch_pae(tups_ctx* ctx) {
   const int nl2 = d.Nl * d.Nl;
   for (int fam = 0; fam < 2; fam++) {
     const int mc = ctx->pae_max_tiles[fam];
-    // tile configs measured on a B200: 8 warps x 32 elements at Nl^2 <= 32
-    // (8x8 / Nl = 5: 1.83 ms), 8 warps x 32 elements x 96 columns with two
-    // CTAs per SM beyond (16x16 / Nl = 9: 482 ms; one 16-warp CTA of 64
-    // elements per SM 540 ms, 64 elements x 48 columns in two chunks 491 ms)
+    // tile configs measured on a B200: 8 warps x 32 elements throughout; at
+    // Nl^2 = 81, 96 columns with two CTAs per SM (16x16 / Nl = 9: 482 ms; one
+    // 16-warp CTA of 64 elements per SM 540 ms, 64 elements x 48 columns in
+    // two chunks 491 ms)
     if (nl2 <= 8) rc = run_pae<1, 1, 4, 2>(ctx, P, 1, fam, mc);
+    // Nl^2 = 25: three IBZ momenta side by side in the columns, 75 of 80
+    // used instead of 25 of 32 (8x8 / Nl = 5: 1.76 ms against 1.89 ms)
+    else if (3 * nl2 <= 80) rc = run_pae<5, 2, 4, 2, 3>(ctx, P, 1, fam, mc);
     else if (nl2 <= 32) rc = run_pae<2, 2, 4, 2>(ctx, P, 1, fam, mc);
     else rc = run_pae<6, 2, 4, 2>(ctx, P, (nl2 + 95) / 96, fam, mc);
     if (rc) return rc;
