@@ -37,7 +37,7 @@ def _check(errs):
     dict(beta=2.0, U=2.0, nParticle=0.9, Nx=4, Nf=8, neighbours=2, Ngrain=3),      # coarse graining
     dict(beta=2.0, U=2.0, nParticle=1.0, Nx=4, Nf=8, neighbours=2, use_U2=False),  # no U^2 term
     dict(beta=10.0, U=3.0, nParticle=0.85, Nx=16, Nf=8, neighbours=3, tprime=-0.2),  # 16x16 k, 9 FF
-    dict(beta=3.0, U=2.0, nParticle=0.9, Nx=4, Nf=64, neighbours=1),  # Nz = 64: the 64 x 64 BSE tiles
+    dict(beta=3.0, U=2.0, nParticle=0.9, Nx=4, Nf=64, neighbours=1),  # Nz = 64: two BSE tiles per dimension
 ], ids=["nl1", "nl5_n09", "nl9_tprime", "frange1", "ngrain3", "noU2", "nx16_nl9", "nz64"])
 def test_phases_side_by_side(gpu_lib, case):
     p = O.Params(f_damping=0.5, ite_max=10, **case)

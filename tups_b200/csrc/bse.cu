@@ -411,17 +411,14 @@ int launch_bse_chunk(tups_ctx* ctx, int q_begin, int q_count) {
     return rc;
   }
   phase_begin(ctx, TUPS_PHASE_BSE_GEMM);
-  // tile choice: 64x64 when Nz is a multiple of 64 (or large), else 32x32;
-  // measured on a B200: 8 warps of 32 x 16 at 64 x 64 with four real
-  // products per complex one (16x16 / Nl = 9: 541 ms against 574 ms with
-  // 4 warps of 32 x 32, 656 ms with three); 32 x 32 tiles with 4 warps and
-  // three real products at Nz = 160 (1.93 ms against 2.13 ms with four;
-  // 2.4-2.8 ms with 4 stages, BK = 32 or 2 warps)
-  if (d.Nz % 64 == 0 || d.Nz > 512) rc = run_gemm<64, 64, 16, 2, 4, 3, false>(ctx, P, q_begin, q_count);
-  // 32 x 32 tiles: two stages (38 KB of shared memory, 5 CTAs per SM by
-  // registers) measured 1.79 ms at 8x8 / Nl = 5 against 1.93 ms with three
-  // stages (57 KB, 4 CTAs per SM) and 2.01 ms with two stages of BK = 32
-  else if (d.Nz >= 32) rc = run_gemm<32, 32, 16, 2, 2, 2, true>(ctx, P, q_begin, q_count);
+  // tile choice, measured on a B200: 32 x 32 tiles of 4 warps (16 x 16 each)
+  // with three real products per complex one on two cp.async stages (38 KB
+  // of shared memory, 5 CTAs per SM by registers) wherever Nz >= 32:
+  // 8x8 / Nl = 5 (Nz = 160) 1.79 ms, against 1.93 ms with three stages,
+  // 2.01 ms with two stages of BK = 32 and 2.13 ms with four products;
+  // 16x16 / Nl = 9 (Nz = 576) 480 ms, against 541 ms for 64 x 64 tiles of
+  // 8 warps (32 x 16 each) with four products and 656 ms with three
+  if (d.Nz >= 32) rc = run_gemm<32, 32, 16, 2, 2, 2, true>(ctx, P, q_begin, q_count);
   else rc = run_gemm<16, 16, 16, 1, 2, 3, true>(ctx, P, q_begin, q_count);
   phase_end(ctx, TUPS_PHASE_BSE_GEMM);
   return rc;
