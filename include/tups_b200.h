@@ -108,9 +108,9 @@ int tups_ctx_destroy(tups_ctx* ctx);
 
 /* Slot-sharded context: rank `rank` of `ntasks` holds the contiguous bosonic
  * slots [rank*Nb, (rank+1)*Nb), Nb = Nred/ntasks, as the reference's MPI ranks
- * do (`Nb = Nred/ntasks`, `id*Nb + idx_q`: SRC/parquet_ini.f90:346-349,
+ * do (`Nb = Nred/ntasks`, `id*Nb + idx_q`: SRC/parquet_ini.f90:336,
  * SRC/preprocessing.f90:98-116); ntasks must divide Nred, as the reference
- * requires (SRC/preprocessing.f90:94-97).  Vertices, chi and the BSE are
+ * requires (SRC/preprocessing.f90:95-98).  Vertices, chi and the BSE are
  * local; Phi(R), Sigma and mu are replicated.  The three steps that need
  * every slot call the exchange function set by tups_set_exchange: the
  * Phi(R) partial sums over the rank's momenta (communicatePhis /

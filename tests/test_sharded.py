@@ -1,6 +1,6 @@
 """Slot sharding on the CPU: the reference's split of the Nred bosonic slots
-over ranks (Nb = Nred/ntasks, contiguous blocks; SRC/parquet_ini.f90:346-349,
-SRC/preprocessing.f90:94-97) and the exchange of the three all-slot buffers
+over ranks (Nb = Nred/ntasks, contiguous blocks; SRC/parquet_ini.f90:336,
+SRC/preprocessing.f90:95-98) and the exchange of the three all-slot buffers
 over two gloo ranks."""
 from __future__ import annotations
 

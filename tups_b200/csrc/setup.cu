@@ -736,8 +736,8 @@ static void free_all(tups_ctx* ctx) {
   ctx->stream = nullptr;
 }
 
-// Slots of rank `rank` of `ntasks` (SRC/parquet_ini.f90:346-349,
-// SRC/preprocessing.f90:94-116): Nb = Nred / ntasks contiguous slots from
+// Slots of rank `rank` of `ntasks` (SRC/parquet_ini.f90:336,
+// SRC/preprocessing.f90:95-116): Nb = Nred / ntasks contiguous slots from
 // rank * Nb; ntasks must divide Nred.
 static int shard_slots(tups_ctx* ctx, int rank, int ntasks) {
   tups_dims& d = ctx->d;

@@ -1,8 +1,8 @@
 """Slot-sharded parquet loop over torch.distributed.
 
 The reference distributes the Nred bosonic slots over its MPI ranks in
-contiguous blocks of Nb = Nred / ntasks (SRC/parquet_ini.f90:346-349,
-SRC/preprocessing.f90:94-116).  A sharded ``Solver`` keeps that split: its
+contiguous blocks of Nb = Nred / ntasks (SRC/parquet_ini.f90:336,
+SRC/preprocessing.f90:95-116).  A sharded ``Solver`` keeps that split: its
 vertices, chi and BSE cover its own slots, and three buffers are combined
 over the ranks during an iteration (the exchange function of the C ABI):
 
