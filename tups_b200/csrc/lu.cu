@@ -6,8 +6,8 @@
 //
 // One persistent launch: each CTA takes the next instance from an atomic
 // counter (instances queued largest first), forms A = I - c Gamma chi (cost
-// n^2 Nl), factors P A = L U with partial pivoting (blocked, panel width 16,
-// trailing rank-16 updates on the FP64 tensor cores), and solves L U F = P
+// n^2 Nl), factors P A = L U with partial pivoting (blocked, panel width 32,
+// trailing rank-32 updates on the FP64 tensor cores), and solves L U F = P
 // Gamma in place for all n right-hand sides.  Caller-owned buffers only; the
 // instance table lives in a static device array.
 #include <algorithm>
@@ -23,7 +23,7 @@ using tups::cplx;
 using tups::cmk;
 
 constexpr int kLuMaxInst = 16384;
-constexpr int NB = 16;
+constexpr int NB = 32;
 constexpr int LU_THREADS = 256;
 
 struct LuDesc {
@@ -48,7 +48,7 @@ __device__ __forceinline__ void dmma8(double* c, const double* a, const double* 
       : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
 
-// C[m x p] -= A[m x K] B[K x p], K <= 16, column-major with leading dim ld
+// C[m x p] -= A[m x K] B[K x p], K <= NB, column-major with leading dim ld
 // (all three inside the same n x n matrix or RHS block).  Warp tiles of
 // 16 x 32 on the FP64 tensor cores, fragments straight from global memory.
 __device__ void rank_update(cplx* C, const cplx* A, const cplx* B, int m, int p, int K, int ldc, int lda, int ldb) {
