@@ -111,9 +111,6 @@ __device__ __forceinline__ void dmma_16x8x8(double* c, const double* a, const do
       : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
 
-#ifndef PAE_SKIP_PAD
-#define PAE_SKIP_PAD 0
-#endif
 #ifndef PAE_MIN_BLOCKS
 #define PAE_MIN_BLOCKS 3  // CTAs per SM asked of ptxas for the 8-warp, <= 2 n-tile configs (2 beyond)
 #endif
@@ -280,9 +277,6 @@ __global__ void __launch_bounds__(32 * RW * WN, RW * WN == 8 ? (TN <= 2 ? PAE_MI
   const int tgt = (wr * 16) / E;            // the warp's target channel
   const int er = (wr * 16) % E + gid;       // its elements er and er + 8
   const double fa = fac[0][tgt], fb = fac[1][tgt];
-#if PAE_SKIP_PAD
-  const int ncols = nl2 - chunk * BN;  // valid columns of this chunk
-#endif
   const bool tr0 = e_tr[er] != 0, tr1 = e_tr[er + 8] != 0;
   double cre[TN][4], cim[TN][4];
 #pragma unroll
@@ -330,9 +324,6 @@ __global__ void __launch_bounds__(32 * RW * WN, RW * WN == 8 ? (TN <= 2 ? PAE_MI
       for (int x = 0; x < 4; x++) anim[x] = -aim[x];
 #pragma unroll
       for (int j = 0; j < TN; j++) {
-#if PAE_SKIP_PAD
-        if ((wc * TN + j) * 8 >= ncols) continue;  // n8 tile wholly past column Nl^2
-#endif
         const int nb = (wc * TN + j) * 8 + gid;
         const cplx w0 = cB[nb * PAE_LDB + k8 + tig], w1 = cB[nb * PAE_LDB + k8 + tig + 4];
         const double bre[2] = {w0.x, w1.x}, bim[2] = {w0.y, w1.y};
