@@ -97,7 +97,9 @@ typedef struct tups_ctx tups_ctx;
 
 /* ---- setup ------------------------------------------------------------ */
 /* set_parameters: parse the 21-record prms file (SRC/parquet_ini.f90:289-324).
- * t' and conv_abs are set to 0. */
+ * t' and conv_abs come from the optional file `<path>.gpu` (`key = value`
+ * lines, keys tprime and conv_abs, `!` or `#` comments), else 0; an unknown
+ * key or a bad value there returns TUPS_ERR_IO. */
 int tups_read_prms(const char* path, tups_params* out);
 /* Initialization + FF_array + do_preprocessing's vertex init
  * (SRC/parquet_util.f90:14-478, SRC/parquet_formfactors.f90:11-90,

@@ -27,6 +27,7 @@ The reference runs with one MPI task here, so ``Nb = Nred``,
 from __future__ import annotations
 
 import math
+import os
 import re
 from dataclasses import dataclass, field
 
@@ -105,14 +106,37 @@ def _f_logical(tok: str) -> bool:
     raise ValueError(f"not a Fortran logical: {tok!r}")
 
 
-def read_prms(path: str, tprime: float = 0.0, conv_abs: float = 0.0) -> Params:
-    """``set_parameters`` (parquet_ini.f90:289-324): one item per record."""
+def read_prms_extras(path: str) -> dict:
+    """The optional ``<prms>.gpu`` file beside the reference's prms (no
+    counterpart in the reference): ``key = value`` lines, ``!`` or ``#``
+    comments, keys tprime and conv_abs; an unknown key or a bad value raises."""
+    out = {"tprime": 0.0, "conv_abs": 0.0}
+    if not os.path.exists(path):
+        return out
+    with open(path) as fh:
+        for ln in fh.read().splitlines():
+            for c in "!#":
+                ln = ln.split(c, 1)[0]
+            f = ln.replace("=", " ").split()
+            if not f:
+                continue
+            if len(f) != 2 or f[0].lower() not in out:
+                raise ValueError(f"{path}: bad line {ln!r}")
+            out[f[0].lower()] = _f_real(f[1])
+    return out
+
+
+def read_prms(path: str, tprime: float | None = None, conv_abs: float | None = None) -> Params:
+    """``set_parameters`` (parquet_ini.f90:289-324): one item per record;
+    ``<path>.gpu`` (``read_prms_extras``) for t' and conv_abs, which keyword
+    values given here override."""
     with open(path) as fh:
         lines = [ln for ln in fh.read().splitlines()]
     lines = [ln for ln in lines if ln.strip()]
     if len(lines) < 21:
         raise ValueError(f"prms file {path} has {len(lines)} records, needs 21")
     tok = [_fortran_token(ln) for ln in lines[:21]]
+    ext = read_prms_extras(str(path) + ".gpu")
     return Params(beta=_f_real(tok[0]), U=_f_real(tok[1]), nParticle=_f_real(tok[2]),
                   Nx=int(tok[3]), Nf=int(tok[4]), neighbours=int(tok[5]),
                   readinpick=_f_logical(tok[6]), pick_file=tok[7], Ngrain=int(tok[8]),
@@ -120,7 +144,8 @@ def read_prms(path: str, tprime: float = 0.0, conv_abs: float = 0.0) -> Params:
                   DGA=_f_logical(tok[12]), fname_L=tok[13], use_sig_dmft=_f_logical(tok[14]),
                   fname_sig_dmft=tok[15], use_U2=_f_logical(tok[16]), save_F=_f_logical(tok[17]),
                   oneshot=_f_logical(tok[18]), old=_f_logical(tok[19]), SDE_old=_f_logical(tok[20]),
-                  tprime=tprime, conv_abs=conv_abs)
+                  tprime=ext["tprime"] if tprime is None else tprime,
+                  conv_abs=ext["conv_abs"] if conv_abs is None else conv_abs)
 
 
 # --------------------------------------------------------------------------

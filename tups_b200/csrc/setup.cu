@@ -396,6 +396,35 @@ int upload(tups_ctx* ctx, T** ptr, const std::vector<T>& v) {
     if (_rc != TUPS_OK) return _rc; \
   } while (0)
 
+// Optional extensions beside the reference's prms (no counterpart in the
+// reference, whose 21 records stay as they are): `<prms>.gpu`, one
+// `key = value` (or `key value`) per line, `!` or `#` starts a comment.
+// Keys: tprime (the t' hopping), conv_abs (sup-norm convergence threshold on
+// dSigma).  An absent file leaves both 0; an unknown key or a bad value is an
+// error, so a misspelt key is not silently ignored.
+static int read_prms_extras(const std::string& path, tups_params* p) {
+  std::ifstream in(path);
+  if (!in) return TUPS_OK;
+  std::string line;
+  while (std::getline(in, line)) {
+    const size_t c = line.find_first_of("!#");
+    if (c != std::string::npos) line.resize(c);
+    for (auto& ch : line)
+      if (ch == '=') ch = ' ';
+    std::istringstream ls(line);
+    std::string key, val, extra;
+    if (!(ls >> key)) continue;
+    if (!(ls >> val) || (ls >> extra)) return TUPS_ERR_IO;
+    for (auto& ch : key) ch = (char)std::tolower((unsigned char)ch);
+    double v;
+    if (!parse_real(val, &v)) return TUPS_ERR_IO;
+    if (key == "tprime") p->tprime = v;
+    else if (key == "conv_abs") p->conv_abs = v;
+    else return TUPS_ERR_IO;
+  }
+  return TUPS_OK;
+}
+
 extern "C" int tups_read_prms(const char* path, tups_params* out) {
   if (!path || !out) return TUPS_ERR_BADARG;
   std::ifstream in(path);
@@ -423,6 +452,8 @@ extern "C" int tups_read_prms(const char* path, tups_params* out) {
   std::snprintf(p.pick_file, sizeof(p.pick_file), "%s", items[7].c_str());
   std::snprintf(p.fname_L, sizeof(p.fname_L), "%s", items[13].c_str());
   std::snprintf(p.fname_sig_dmft, sizeof(p.fname_sig_dmft), "%s", items[15].c_str());
+  const int rc = read_prms_extras(std::string(path) + ".gpu", &p);
+  if (rc) return rc;
   *out = p;
   return TUPS_OK;
 }

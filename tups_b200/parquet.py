@@ -93,15 +93,20 @@ def _check(lib, ctx, rc: int) -> None:
         raise TupsError(rc, msg or lib.tups_strerror(rc).decode())
 
 
-def read_prms(path: str, tprime: float = 0.0, conv_abs: float = 0.0) -> Params:
-    """``set_parameters``: parse a 21-record prms file with the native parser."""
+def read_prms(path: str, tprime: float | None = None, conv_abs: float | None = None) -> Params:
+    """``set_parameters``: parse a 21-record prms file with the native parser,
+    and ``<path>.gpu`` (tprime, conv_abs) when it exists; keyword values given
+    here take precedence over that file."""
     lib = _lib.load()
     p = tups_params()
     rc = lib.tups_read_prms(str(path).encode(), C.byref(p))
     if rc != 0:
-        raise TupsError(rc, f"cannot read prms file {path}")
+        raise TupsError(rc, f"cannot read prms file {path} (or its .gpu extensions)")
     out = Params.from_c(p)
-    out.tprime, out.conv_abs = tprime, conv_abs
+    if tprime is not None:
+        out.tprime = tprime
+    if conv_abs is not None:
+        out.conv_abs = conv_abs
     return out
 
 
