@@ -419,6 +419,33 @@ class Solver:
         a = np.asfortranarray(v, dtype=np.complex128)
         self._call("tups_set_vertex", ch, which, _ptr(a))
 
+    def save_state(self, path, ite: int) -> None:
+        """Checkpoint for a resume in another process: Sigma, mu and the
+        vertices F_r and G_r (Gamma_r after the vertex update) to an ``.npz``
+        file, with ``ite``, the next iteration to run.  Every other piece of
+        device state is recomputed by the next iteration (Phi(R), the phase
+        tables and the crossing tensors on the first iteration of a new
+        context), so a resumed loop repeats the uninterrupted one bit for bit;
+        only the first conv after it reports no change of max|F_r| (that
+        comparison is host state).  Holds 8 Nz^2 Nb complex values in host
+        memory."""
+        np.savez(path, ite=ite, Sigma=self.Sigma, mu=self.mu,
+                 F=np.stack([self.F(r) for r in CHANNELS]), G=np.stack([self.G(r) for r in CHANNELS]),
+                 shape=np.array([self.Nz, self.Nb, self.Nt, self.slot0]))
+
+    def load_state(self, path) -> int:
+        """Restore a ``save_state`` file into this context (same parameters and
+        slots); returns the iteration to run next."""
+        d = np.load(path)
+        if tuple(d["shape"]) != (self.Nz, self.Nb, self.Nt, self.slot0):
+            raise ValueError(f"{path} holds a state of other sizes {tuple(d['shape'])}")
+        self.Sigma = d["Sigma"]
+        self.mu = float(d["mu"])
+        for i, r in enumerate(CHANNELS):
+            self.set_vertex(r, 0, d["F"][i])
+            self.set_vertex(r, 1, d["G"][i])
+        return int(d["ite"])
+
     def PhiR(self, channel) -> np.ndarray:
         ch = CHANNELS.index(channel) if isinstance(channel, str) else int(channel)
         a = np.empty((self.Nz * self.Nz, self.Nf // 2, self.NR), dtype=np.complex128, order="F")
