@@ -21,6 +21,8 @@
 #ifndef TUPS_B200_H
 #define TUPS_B200_H
 
+#include <stddef.h> /* size_t */
+
 #ifdef __cplusplus
 extern "C" {
 #endif

@@ -85,3 +85,17 @@ def test_host_tables_reject_bad_sizes(gpu_lib):
         host_tables(Params(Nx=4, Nf=15))
     with pytest.raises(TupsError):
         host_tables(Params(Nx=4, Nf=16, old=True))
+
+
+@pytest.mark.parametrize("lang,std", [("c", "-std=c99"), ("c++", "-std=c++17")])
+def test_header_compiles_on_its_own(lang, std):
+    """A C or C++ host includes include/tups_b200.h with nothing before it."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") if lang == "c" else shutil.which("g++")
+    if cc is None:
+        pytest.skip("no host compiler")
+    hdr = Path(__file__).resolve().parents[1] / "include" / "tups_b200.h"
+    r = subprocess.run([cc, "-fsyntax-only", "-Wall", "-Wextra", "-Werror", std, "-x", lang, str(hdr)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
