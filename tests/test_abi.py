@@ -99,3 +99,35 @@ def test_header_compiles_on_its_own(lang, std):
     r = subprocess.run([cc, "-fsyntax-only", "-Wall", "-Wextra", "-Werror", std, "-x", lang, str(hdr)],
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+def test_c_host_links_and_reads_prms(gpu_lib, tmp_path):
+    """A C program linked against libtups_b200.so parses a prms file and gets
+    the derived sizes from the host tables, as a compiled host would (no GPU
+    needed for these two calls)."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc")
+    if cc is None:
+        pytest.skip("no host compiler")
+    root = Path(__file__).resolve().parents[1]
+    src = tmp_path / "host.c"
+    src.write_text(
+        '#include <stdio.h>\n#include "tups_b200.h"\n'
+        "int main(int argc, char** argv) {\n"
+        "  tups_params p; tups_dims d;\n"
+        "  int rc = tups_read_prms(argv[1], &p);\n"
+        "  if (!rc) rc = tups_host_tables(&p, &d, 0, 0, 0, 0, 0, 0, 0);\n"
+        "  if (rc) { printf(\"error %d %s\\n\", rc, tups_strerror(rc)); return 1; }\n"
+        '  printf("%d %d %d %d %d\\n", d.Nl, d.Nz, d.Nred, d.NIBZ, d.NR);\n'
+        "  return 0;\n}\n")
+    exe = tmp_path / "host"
+    lib_dir = root / "tups_b200"
+    r = subprocess.run([cc, "-std=c99", "-Wall", "-Werror", f"-I{root / 'include'}", str(src), f"-L{lib_dir}",
+                        "-ltups_b200", f"-Wl,-rpath,{lib_dir}", "-o", str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    for name in ("pa_4x4_nl1", "pa_4x4_nl5"):
+        out = subprocess.run([str(exe), str(GOLD / f"prms_{name}")], capture_output=True, text=True, timeout=60)
+        assert out.returncode == 0, out.stdout + out.stderr
+        st = O.initialize(O.read_prms(str(GOLD / f"prms_{name}")))
+        assert [int(x) for x in out.stdout.split()] == [st.Nl, st.Nz, st.Nred, st.NIBZ, st.NR]
