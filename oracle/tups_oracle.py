@@ -9,8 +9,9 @@ ships no golden vectors and cannot be compiled in this image (no Fortran
 compiler).  This module restates it function by function; every function
 cites the reference file:line it follows.  It is pinned only by the
 reference's own inline known-answer checks (``FF_sdwave_check``,
-form-factor orthogonality) and by physics invariants, see
-``tests/test_oracle_invariants.py``.
+form-factor orthogonality, ``check_chi0``) and by physics invariants (U = 0,
+second order, point-group, particle-hole and conjugation symmetry), see
+``tests/test_oracle.py``.
 
 Array conventions follow the reference exactly, with 0-based indices:
 
