@@ -157,7 +157,9 @@ const char* tups_strerror(int status);
  * readout branch (:216-430) is not part of this call. */
 int tups_calc_Gkw_Grt(tups_ctx* ctx, int ite, int cal_chi);
 /* calc_chi(map_q, chi_ph_LL, chi_pp_LL) (SRC/parquet_chi.f90:438-523) for the
- * 1-based bosonic IBZ slot idx_q; writes the dense (Nz,Nz) matrices to host. */
+ * 1-based bosonic IBZ slot idx_q of this context (1..Nb; in a sharded context
+ * global slot slot0 + idx_q, as the reference's id*Nb + idx_q); writes the
+ * dense (Nz,Nz) matrices to host. */
 int tups_calc_chi(tups_ctx* ctx, int idx_q, double* chi_ph_LL, double* chi_pp_LL);
 
 /* ---- module Parquet_kernel ------------------------------------------- */
