@@ -209,6 +209,12 @@ int tups_set_graph(tups_ctx* ctx, int enable);
  * iteration (SRC/loop.f90:181-213; results via tups_get_chi0/tups_get_sus);
  * *ite_out = iterations done */
 int tups_execute_loop(tups_ctx* ctx, int* ite_out, int* converged);
+/* One iteration of execute_loop with its output block (SRC/loop.f90:181-213):
+ * at iterations ite % 5 == 0, ite_max - 1 and on convergence the readout
+ * (tups_readout) runs after conv and before the vertex update, as in the
+ * reference, and its results stay readable (tups_get_chi0, tups_get_sus)
+ * until the next readout.  Unsharded contexts only. */
+int tups_iteration_readout(tups_ctx* ctx, int ite, tups_conv_info* info);
 
 /* ---- warm start and checkpoint ----------------------------------------------
  * Warm start at the reference's initialisation hook (SRC/preprocessing.f90:100-116,

@@ -1620,8 +1620,12 @@ def output_block_mu(st: State) -> None:
     st.mu = 0.5 * ((st.mu + p.U) + (st.mu - p.U))
 
 
-def iteration(st: State, ite: int) -> tuple[bool, dict]:
-    """One pass of ``execute_loop`` (loop.f90:51-244) without the HDF5 output."""
+def iteration(st: State, ite: int, with_readout: bool = False) -> tuple[bool, dict]:
+    """One pass of ``execute_loop`` (loop.f90:51-244) without the HDF5 output.
+    ``with_readout``: at the output iterations run the readout of the output
+    block (loop.f90:181-213) where the reference does, after conv and before
+    the vertex update, and return it as ``info["readout"]``; its
+    calc_Gkw_Grt(.true.) has the same effect on mu as ``output_block_mu``."""
     p = st.p
     steps = calc_Gkw_Grt(st, ite, False)
     bse(st, ite)
@@ -1639,7 +1643,10 @@ def iteration(st: State, ite: int) -> tuple[bool, dict]:
     info["bisection_steps"] = steps
     info["mu"] = st.mu
     if ite % 5 == 0 or ite == p.ite_max - 1 or converged:
-        output_block_mu(st)
+        if with_readout:
+            info["readout"] = readout(st, ite)
+        else:
+            output_block_mu(st)
     for r in "dmst":
         st.G[r] = st.F[r] - st.G[r]
     return converged, info

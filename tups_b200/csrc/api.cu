@@ -427,6 +427,15 @@ static int iteration_graph(tups_ctx* ctx, int ite, tups_conv_info* info) {
   return TUPS_OK;
 }
 
+// one iteration with the readout of the output block at the reference's
+// output iterations (every 5th, the last, on convergence), after conv and
+// before the vertex update, as each step of tups_execute_loop does
+extern "C" int tups_iteration_readout(tups_ctx* ctx, int ite, tups_conv_info* info) {
+  if (ctx && ctx->ntasks > 1)
+    return tups::set_error(ctx, TUPS_ERR_STATE, "the readout needs every slot: use an unsharded context");
+  return iteration_impl(ctx, ite, info, true);
+}
+
 extern "C" int tups_set_graph(tups_ctx* ctx, int enable) {
   if (!ctx) return TUPS_ERR_BADARG;
   ctx->use_graph = enable != 0;

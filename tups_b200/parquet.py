@@ -266,9 +266,13 @@ class Solver:
     def output_block(self) -> None:
         self._call("tups_output_block")
 
-    def iteration(self, ite: int) -> dict:
+    def iteration(self, ite: int, readout: bool = False) -> dict:
+        """One iteration of execute_loop.  ``readout``: also the output block's
+        readout at the output iterations (every 5th, the last, on
+        convergence), after conv and before the vertex update as in the
+        reference; ``chi0(bz)`` and ``sus(r, bz)`` then hold its results."""
         ci = tups_conv_info()
-        self._call("tups_iteration", int(ite), C.byref(ci))
+        self._call("tups_iteration_readout" if readout else "tups_iteration", int(ite), C.byref(ci))
         return _conv_dict(ci)
 
     def execute_loop(self) -> tuple[int, bool]:
