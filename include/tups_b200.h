@@ -145,6 +145,11 @@ int tups_get_shard(const tups_ctx* ctx, int* rank, int* ntasks, int* slot0);
  * form-factor / symmetry / index tables in the layouts of tups_get_tables.
  * Lets a caller size its host arrays before creating a context. Any output
  * pointer may be NULL. */
+/* The DGA branch of Initialization (SRC/parquet_util.f90:317-346) without a
+ * device: reads `<fname_L>_ph.init` (Lambda_d, Lambda_m) and `_pp.init`
+ * (Lambda_s, Lambda_t) into (Nf, Nf, Nf/2) complex arrays, the tables a DGA
+ * context starts from.  Any output pointer may be NULL. */
+int tups_read_lambda(const char* fname_L, int Nf, double* L_d, double* L_m, double* L_s, double* L_t);
 int tups_host_tables(const tups_params* p, tups_dims* d, double* FF, double* FF_inv, int* signs, int* reps,
                      int* lsym, double* lfac, int* ibz);
 int tups_get_dims(const tups_ctx* ctx, tups_dims* out);

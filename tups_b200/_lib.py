@@ -62,6 +62,7 @@ _PROTOS = {
     "tups_ctx_create_sharded": [C.POINTER(tups_params), C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p)],
     "tups_set_exchange": [C.c_void_p, C.c_void_p, C.c_void_p],
     "tups_iteration_readout": [C.c_void_p, C.c_int, C.c_void_p],
+    "tups_read_lambda": [C.c_char_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
     "tups_get_shard": [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)],
     "tups_ctx_destroy": [C.c_void_p],
     "tups_host_tables": [C.POINTER(tups_params), C.POINTER(tups_dims)] + [C.c_void_p] * 7,

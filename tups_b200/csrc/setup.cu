@@ -808,6 +808,20 @@ static int ctx_create(const tups_params* p, int device, int rank, int ntasks, tu
   return TUPS_OK;
 }
 
+extern "C" int tups_read_lambda(const char* fname_L, int Nf, double* L_d, double* L_m, double* L_s,
+                                double* L_t) {
+  if (!fname_L || Nf < 2 || Nf % 2) return TUPS_ERR_BADARG;
+  std::vector<cplx> L[4];
+  const std::string base = trim_name(fname_L);
+  int rc = read_lambda_file(nullptr, base + "_ph.init", Nf, L[0], L[1]);
+  if (!rc) rc = read_lambda_file(nullptr, base + "_pp.init", Nf, L[2], L[3]);
+  if (rc) return rc;
+  double* out[4] = {L_d, L_m, L_s, L_t};
+  for (int r = 0; r < 4; r++)
+    if (out[r]) std::memcpy(out[r], L[r].data(), L[r].size() * sizeof(cplx));
+  return TUPS_OK;
+}
+
 extern "C" int tups_ctx_create(const tups_params* p, int device, tups_ctx** out) {
   return ctx_create(p, device, 0, 1, out);
 }
