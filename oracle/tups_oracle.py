@@ -1426,7 +1426,8 @@ def conv(st: State) -> tuple[bool, dict]:
     """``conv`` (parquet_check.f90:39-150), plus the optional absolute
     sup-norm test on the self-energy change."""
     S, So = st.Sigma, st.SigmaOld
-    rel = np.abs(So - S) / np.abs(S)
+    with np.errstate(invalid="ignore", divide="ignore"):  # Sigma = 0 (U = 0): NaN, as in the reference
+        rel = np.abs(So - S) / np.abs(S)
     rel_sig_max = float(np.max(rel))
     dsig_inf = float(np.max(np.abs(So - S)))
     out = {"rel_sig_max": rel_sig_max, "rel_sig_av": float(abs(np.sum(rel) / rel.size)),
