@@ -207,23 +207,47 @@ def blas_threads() -> int:
     return os.cpu_count() or 1
 
 
+def workload_config(wl_name: str, wl: dict, ws: int) -> dict:
+    """The `config` record, identical in both arms: the prms fields, the
+    derived sizes (from the host-side tables, no device needed) and the L2
+    statement."""
+    from tups_b200 import Params
+    from tups_b200.parquet import host_tables
+    d = host_tables(Params(**{k: v for k, v in wl.items() if k in Params.__dataclass_fields__}))["dims"]
+    Nz, Nb = d["Nz"], d["Nb"]
+    return {"workload": wl_name, **{k: wl[k] for k in ("Nx", "Nf", "neighbours", "beta", "U", "nParticle")},
+            "tprime": wl.get("tprime", 0.0), "Nl": d["Nl"], "Nz": Nz, "Nred": d["Nred"], "NR": d["NR"],
+            "l2": "resident state ~%.2f GB > 126 MB L2; no flush" % ((8 * Nz * Nz * Nb * 16) / 1e9),
+            "parallelism": "replicas" if ws > 1 else "single process"}
+
+
+def fortran_toolchain() -> dict:
+    """Which Fortran/MPI compilers this host has (the reference needs mpif90,
+    MKL and HDF5-Fortran)."""
+    import shutil
+    return {t: shutil.which(t) for t in ("gfortran", "mpif90", "mpifort", "ifort", "ifx", "h5fc")}
+
+
 def run_reference(args, wl_name: str, wl: dict):
     ws, rank, _ = dist_env()
     if rank != 0:
         return
-    steps = max(1, min(args.steps, 3))
-    warm = 1
+    steps, warm = args.steps, args.warmup
     spi = cpu_oracle_seconds_per_iteration(wl, timed_iterations=steps, warm_iterations=warm)
     cores = blas_threads()
+    tools = fortran_toolchain()
     line = {
         "impl": "reference", "metric": METRIC, "metric_full": METRIC_FULL, "value": spi, "unit": "s/iter",
         "n_gpus": ws, "steps": steps, "warmup": warm, "ms_per_step": spi * 1e3, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": wl_name, **{k: wl[k] for k in ("Nx", "Nf", "neighbours", "beta", "U", "nParticle")},
-                   "parallelism": "host cores"},
+        "config": workload_config(wl_name, wl, ws),
         "cpu_baseline": {"value": spi, "unit": "s/iter", "cores": cores, "kind": "port",
                          "sample": f"{steps} oracle iteration(s) after {warm} untimed; numpy/OpenBLAS "
-                                   "restatement (the Fortran reference has no compiler in this image)"},
+                                   "restatement of the reference"},
+        "reference_toolchain": tools,
+        "reference_note": ("the Fortran reference needs mpif90 + MKL + HDF5-Fortran; none of the compilers "
+                           "probed here is present" if not any(tools.values()) else
+                           "a Fortran compiler is present; the port is still the timed arm"),
         "e2e": {"value": spi, "unit": "s/iter", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -334,6 +358,10 @@ def run_tups(args, wl_name: str, wl: dict):
         graph = graph_iterations(params, device, K, W)
     if ws == 1 and (Nz <= 256 or args.convergence) and not args.no_convergence:
         conv = to_convergence(params, device)
+    target = None
+    if ws == 1 and not args.no_target and wl_name != TARGET_WORKLOAD:
+        sol.close()
+        target = target_record(device)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         sec = cpu_oracle_seconds_per_iteration(wl)
@@ -346,16 +374,12 @@ def run_tups(args, wl_name: str, wl: dict):
             "steps": K, "warmup": W, "ms_per_step": ms / K, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if not args.bse_slices else f"f64 + int8x{args.bse_slices} BSE GEMM",
             "data": "synthetic",
-            "config": {"workload": wl_name,
-                       **{k: wl[k] for k in ("Nx", "Nf", "neighbours", "beta", "U", "nParticle")},
-                       "tprime": wl.get("tprime", 0.0), "Nl": d["Nl"], "Nz": Nz, "Nred": d["Nred"], "NR": NR,
-                       "l2": "resident state ~%.2f GB > 126 MB L2; no flush" % (
-                           (8 * Nz * Nz * Nb * 16) / 1e9),
-                       "parallelism": "replicas" if ws > 1 else "single GPU"},
+            "config": workload_config(wl_name, wl, ws),
             "bse_tflops": bse_tflops,
             "split_precision": split,
             "cuda_graph": graph,
             "to_convergence": conv,
+            "target": target,
             "roofline": roof,
             "kernels": kern,
             "phase_ms_per_iter": {p: v[0] / K for p, v in phases.items()},
@@ -428,17 +452,44 @@ def graph_iterations(params, device: int, K: int, W: int) -> dict:
     return {"ms_per_iter": ms, "kernels_per_iter": launches}
 
 
-def to_convergence(params, device: int, max_iter: int = 3000) -> dict:
+def _final_state(sol, n: int, full_vertices: bool, sample_slots) -> dict:
+    """One more iteration of a converged loop with the readout (outside any
+    timed region): Sigma, F_r, Gamma_r (after the vertex update), chi0 and
+    sus_r.  Large grids keep only the sampled slots of the vertices."""
+    sol.iteration(n, readout=True)
+    out = {"Sigma": sol.Sigma}
+    for r in "dmst":
+        if full_vertices:
+            out["F_" + r] = sol.F(r)
+            out["Gamma_" + r] = sol.G(r)
+        else:
+            out["F_" + r] = np.stack([sol.vertex_slots(r, 0, q)[:, :, 0] for q in sample_slots])
+            out["Gamma_" + r] = np.stack([sol.vertex_slots(r, 1, q)[:, :, 0] for q in sample_slots])
+        out["sus_" + r] = sol.sus(r)
+    out.update(sol.chi0())
+    return out
+
+
+def _rel(a, b) -> float:
+    den = float(np.max(np.abs(b)))
+    return float(np.max(np.abs(a - b))) / den if den > 0 else float(np.max(np.abs(a - b)))
+
+
+def to_convergence(params, device: int, max_iter: int = 3000, graph: bool = True) -> dict:
     """Wall time (device events around the host-driven loop) and iterations to
     max|dSigma| < 1e-10 from the reference's initial state: FP64 BSE vs the
-    precision ladder; Sigma of the ladder run against the FP64 run."""
+    precision ladder, both replaying CUDA graphs.  Then the converged states
+    against each other, max-norm relative error per quantity: Sigma, F_r and
+    Gamma_r of each channel, the chi0 bubble and the susceptibilities sus_r
+    of the readout (the FP64 path equals the oracle to 1e-12 per phase)."""
     from dataclasses import replace
     from tups_b200 import Solver
     p = replace(params, conv_abs=1e-10, ite_max=10 ** 6)
     res = {}
-    sig = {}
+    fin = {}
     for name in ("fp64", "ladder"):
         sol = Solver(p, device=device)
+        sol.set_graph(graph)
         if name == "ladder":
             sol.set_bse_precision(0, ladder=True)
         used = []
@@ -454,15 +505,49 @@ def to_convergence(params, device: int, max_iter: int = 3000) -> dict:
                 break
         sol.record_event(5)
         sec = sol.event_elapsed_ms(4, 5) * 1e-3
-        sig[name] = sol.Sigma
+        full = sol.Nz * sol.Nz * sol.Nb * 16 * 8 < 4e9
+        slots = [0, sol.Nb // 2, sol.Nb - 1]
+        fin[name] = _final_state(sol, n, full, slots)
         sol.close()
-        res[name] = {"iterations": n, "seconds": sec, "converged": ok}
+        res[name] = {"iterations": n, "seconds": sec, "s_per_iter": sec / n, "converged": ok}
         if name == "ladder":
             res[name]["slices_per_iteration"] = used
-    a, b = sig["ladder"], sig["fp64"]
-    res["sigma_rel_err_ladder_vs_fp64"] = float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+    a, b = fin["ladder"], fin["fp64"]
+    errs = {k: _rel(a[k], b[k]) for k in b}
+    res["rel_err_ladder_vs_fp64"] = errs
+    res["rel_err_note"] = ("max-norm relative difference of the ladder's converged state from the FP64 one, "
+                           "both stopped at max|dSigma| < 1e-10; vertices " +
+                           ("whole" if full else "at slots [0, Nb/2, Nb-1]") +
+                           "; Gamma_r after the vertex update; chi0/sus from the readout of one more iteration")
+    res["sigma_rel_err_ladder_vs_fp64"] = errs["Sigma"]
     res["speedup_ladder_vs_fp64"] = res["fp64"]["seconds"] / res["ladder"]["seconds"]
+    res["launch_mode"] = "CUDA graph per iteration" if graph else "kernel by kernel"
     return res
+
+
+TARGET_WORKLOAD = "pa_16x16_nl9_nf64"
+
+
+def target_record(device: int) -> dict:
+    """The 16x16 k / 9 form factor / 64 frequency loop (t' = -0.2, n = 0.85,
+    U = 3, beta = 10): FP64 vs precision-ladder time to max|dSigma| < 1e-10
+    and the converged states' difference, with its own clock samples.  The
+    learned warm start is trained on the 8x8 / 5 form-factor grid and has no
+    network for this grid, so the ladder runs from the cold start."""
+    from tups_b200 import Params
+    wl = WORKLOADS[TARGET_WORKLOAD]
+    params = Params(**{k: v for k, v in wl.items() if k in Params.__dataclass_fields__})
+    clocks = ClockSampler(device)
+    clocks.start()
+    t0 = time.perf_counter()
+    conv = to_convergence(params, device)
+    wall = time.perf_counter() - t0
+    clk = clocks.stop()
+    return {"workload": TARGET_WORKLOAD,
+            "config": {k: wl[k] for k in ("Nx", "Nf", "neighbours", "beta", "U", "nParticle", "tprime")},
+            "fp64_s_per_iter": conv["fp64"]["s_per_iter"], "to_convergence": conv, "host_wall_s": wall,
+            "warm_start": "not run: the network is trained on the 8x8 / 5 form-factor grid only",
+            "clocks": clk}
 
 
 LU_WORKLOAD = "bse_lu_1024"
@@ -572,6 +657,8 @@ def main():
     ap.add_argument("--no-convergence", action="store_true", help="skip the runs to convergence")
     ap.add_argument("--convergence", action="store_true",
                     help="also run the loops to convergence when Nz > 256 (minutes at 16x16)")
+    ap.add_argument("--no-target", action="store_true",
+                    help="skip the 16x16 / 9 form factor FP64-vs-ladder record (about 6 minutes)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "tups":
         args.warmup = 3

@@ -145,13 +145,13 @@ int tups_get_shard(const tups_ctx* ctx, int* rank, int* ntasks, int* slot0);
  * form-factor / symmetry / index tables in the layouts of tups_get_tables.
  * Lets a caller size its host arrays before creating a context. Any output
  * pointer may be NULL. */
+int tups_host_tables(const tups_params* p, tups_dims* d, double* FF, double* FF_inv, int* signs, int* reps,
+                     int* lsym, double* lfac, int* ibz);
 /* The DGA branch of Initialization (SRC/parquet_util.f90:317-346) without a
  * device: reads `<fname_L>_ph.init` (Lambda_d, Lambda_m) and `_pp.init`
  * (Lambda_s, Lambda_t) into (Nf, Nf, Nf/2) complex arrays, the tables a DGA
  * context starts from.  Any output pointer may be NULL. */
 int tups_read_lambda(const char* fname_L, int Nf, double* L_d, double* L_m, double* L_s, double* L_t);
-int tups_host_tables(const tups_params* p, tups_dims* d, double* FF, double* FF_inv, int* signs, int* reps,
-                     int* lsym, double* lfac, int* ibz);
 int tups_get_dims(const tups_ctx* ctx, tups_dims* out);
 const char* tups_last_error(const tups_ctx* ctx);
 const char* tups_strerror(int status);
@@ -302,6 +302,12 @@ int tups_set_mu(tups_ctx* ctx, double mu);
  * and the vertex update); layout (Nz, Nz, Nb) */
 int tups_get_vertex(tups_ctx* ctx, int channel, int which, double* host);
 int tups_set_vertex(tups_ctx* ctx, int channel, int which, const double* host);
+/* the same for `count` consecutive slots from the 0-based local slot
+ * `slot_begin` only: (Nz, Nz, count), the F_r/G_r columns a parity dump or the
+ * reference's vertex output of save_F (write_F, SRC/parquet_plot.f90:237-276)
+ * needs without moving the whole (Nz, Nz, Nb) array */
+int tups_get_vertex_slots(tups_ctx* ctx, int channel, int which, int slot_begin, int count, double* host);
+int tups_set_vertex_slots(tups_ctx* ctx, int channel, int which, int slot_begin, int count, const double* host);
 int tups_get_PhiR(tups_ctx* ctx, int channel, double* host);  /* (Nz*Nz, Nf/2, NR) */
 /* which: 0 phbar_to_ph, 1 pp_to_ph, 2 ph_to_pp, 3 phbar_to_pp;
  * layout (Nl, Nl, Nl, Nl, Nb, NR) as M_* of SRC/parquet_EQMatrix.f90:12-16 */
@@ -326,7 +332,7 @@ long long tups_kernel_launches(const tups_ctx* ctx);
  * SRC/parquet_BSE.f90:72-128, whose fixed point this reproduces):
  *   F_i = (1 - scale_i Gamma_i chi_i)^{-1} Gamma_i   (want_phi: F_i - Gamma_i)
  * for n_inst instances of size n[i] = nl[i] * Nnu_i, in one persistent launch
- * (CTAs take instances largest first; partial-pivoting LU, panel 16, FP64
+ * (CTAs take instances largest first; partial-pivoting LU, panel 32, FP64
  * tensor-core trailing updates; n[i] right-hand sides).  n, nl, scale: host
  * arrays.  gamma, out, work: device, instances packed consecutively as
  * (n, n) column-major complex128; chi: device, packed (nl, nl, Nnu) blocks;
@@ -350,8 +356,10 @@ int tups_bse_lu_batched(int n_inst, const int* n, const int* nl, const double* s
  * (c = 1/2, 1/2, -1/4, 1/4 for d, m, s, t); stream: a cudaStream_t or NULL.
  * Limit: Nz <= 1024.  The scratch is a fixed 32 MiB static device array that
  * every GPU loading the library holds until exit; the first call on a device
- * looks up its address (make it before any stream capture); calls that
- * overlap on the GPU race on it.  Allocates nothing; returns after queueing. */
+ * looks up its address (make it before any stream capture) and keeps it for
+ * the life of the process, so do not call this on a device again after a
+ * cudaDeviceReset of it; calls that overlap on the GPU race on it.  Allocates
+ * nothing; returns after queueing. */
 int tups_bse_noalloc(int n_inst, int Nz, int Nf, int Nl, double* gamma_phi, const double* F, const double* chi,
                      double scale, double f_damping, void* stream);
 

@@ -538,10 +538,14 @@ def write_lambda_file(path: str, A: np.ndarray, B: np.ndarray) -> None:
                     fh.write(f"{k1 + 1} {k2 + 1} {q + 1} {a.real:.17e} {a.imag:.17e} {b.real:.17e} {b.imag:.17e}\n")
 
 
-def initialize(p: Params) -> State:
+def initialize(p: Params, vertices: bool = True) -> State:
     """``set_parameters`` derived sizes (parquet_ini.f90:326-349),
     ``Initialization`` (parquet_util.f90:14-478), ``FF_array`` and the
-    vertex initialisation of ``do_preprocessing`` (preprocessing.f90:100-133)."""
+    vertex initialisation of ``do_preprocessing`` (preprocessing.f90:100-133).
+
+    vertices=False skips the (Nz, Nz, Nb) vertex arrays (61 GB on the 16x16 /
+    9 form factor / 64 frequency grid), for the slot-restricted functions
+    ``bse_slot``, ``phir_at_w`` and ``crossing_slot``."""
     if p.Nf % 2:
         raise ValueError("Nf must be even")
     if p.old or p.SDE_old:
@@ -647,7 +651,7 @@ def initialize(p: Params) -> State:
     F = {}
     G = {}
     q0 = ibz[:, 2] - 1
-    for r in "dmst":
+    for r in "dmst" if vertices else "":
         F[r] = np.zeros((st.Nz, st.Nz, st.Nb), dtype=np.complex128, order="F")
         F[r][:Nf, :Nf, :] = Ls[r][:, :, q0] * aux
         G[r] = F[r].copy(order="F")
@@ -905,24 +909,29 @@ def calc_chi(st: State, qx: int, qy: int, w: int) -> tuple[np.ndarray, np.ndarra
 BSE_COEF = {"d": 0.5, "m": 0.5, "s": -0.25, "t": 0.25}  # parquet_BSE.f90:73,89,105,120
 
 
-def bse(st: State, ite: int = 0) -> None:
-    """``BSE(ite)``: the damped two-ordering update; on exit G_r holds Phi_r."""
+def bse_slot(st: State, r: str, Gm: np.ndarray, Fm: np.ndarray, chi: np.ndarray) -> np.ndarray:
+    """The damped two-ordering update of one (q, channel) instance
+    (parquet_BSE.f90:72-128): Phi = c f [(a Gamma chi) F + F (a chi Gamma)]
+    + (1 - f)(F - Gamma), a = 1/(beta Nx Ny)."""
     p = st.p
     alpha = 1.0 / (p.beta * st.Nx * st.Ny)
     f = p.f_damping
+    c = BSE_COEF[r] * f
+    chiG = alpha * (Gm @ chi)
+    gam = c * (chiG @ Fm)
+    chiG = alpha * (chi @ Gm)
+    gam = gam + c * (Fm @ chiG)
+    return gam + (1.0 - f) * (Fm - Gm)
+
+
+def bse(st: State, ite: int = 0) -> None:
+    """``BSE(ite)``: the damped two-ordering update; on exit G_r holds Phi_r."""
     for iq in range(st.Nb):
         qx, qy, w = (int(v) for v in st.ibz[iq])
         cph, cpp = calc_chi(st, qx, qy, w)
         for r in "dmst":
             chi = cph if r in "dm" else cpp
-            Gm = st.G[r][:, :, iq]
-            Fm = st.F[r][:, :, iq]
-            c = BSE_COEF[r] * f
-            chiG = alpha * (Gm @ chi)
-            gam = c * (chiG @ Fm)
-            chiG = alpha * (chi @ Gm)
-            gam = gam + c * (Fm @ chiG)
-            st.G[r][:, :, iq] = gam + (1.0 - f) * (Fm - Gm)
+            st.G[r][:, :, iq] = bse_slot(st, r, st.G[r][:, :, iq], st.F[r][:, :, iq], chi)
 
 
 # --------------------------------------------------------------------------
@@ -985,11 +994,25 @@ def symop_perm(st: State, s: int) -> tuple[np.ndarray, np.ndarray]:
     return src, fac
 
 
+def phir_at_w(st: State, PhiQ_w: np.ndarray, perms=None) -> np.ndarray:
+    """``FTPhis`` (parquet_PhiR.f90:196-258) for one bosonic frequency:
+    PhiQ_w (Nz*Nz, NIBZ), Phi_r of the IBZ momenta at that frequency, column-
+    major per momentum -> Phi_r(R) (Nz*Nz, NR)."""
+    if perms is None:
+        perms = [symop_perm(st, s) for s in range(1, NS + 1)]
+    exps = st.expSqR
+    acc = np.zeros((st.Nz * st.Nz, st.NR), dtype=np.complex128)
+    for s in range(NS):
+        src, fac = perms[s]
+        d1 = fac[:, None] * PhiQ_w[src, :]
+        acc = acc + (1.0 / st.Nx) * (d1 @ exps[:, :, s])
+    return acc
+
+
 def calc_PhiR(st: State) -> None:
     """``calc_PhiR`` -> ``communicatePhis`` (a local copy at one task) ->
     ``FTPhis`` (parquet_PhiR.f90:35-258).  Result PhiR[r] (Nz*Nz, Nf/2, NR)."""
     Nz, Nf, NIBZ = st.Nz, st.Nf, st.NIBZ
-    exps = st.expSqR
     perms = [symop_perm(st, s) for s in range(1, NS + 1)]
     PhiR = {}
     for r in "dmst":
@@ -997,12 +1020,7 @@ def calc_PhiR(st: State) -> None:
         PhiQ = st.G[r].reshape(Nz * Nz, Nf // 2, NIBZ, order="F")
         out = np.zeros((Nz * Nz, Nf // 2, st.NR), dtype=np.complex128)
         for w in range(Nf // 2):
-            acc = np.zeros((Nz * Nz, st.NR), dtype=np.complex128)
-            for s in range(NS):
-                src, fac = perms[s]
-                d1 = fac[:, None] * PhiQ[src, w, :]
-                acc = acc + (1.0 / st.Nx) * (d1 @ exps[:, :, s])
-            out[:, w, :] = acc
+            out[:, w, :] = phir_at_w(st, PhiQ[:, w, :], perms)
         PhiR[r] = out
     st.arrays["PhiR"] = PhiR
 
@@ -1215,6 +1233,51 @@ def calculate_PAE(st: State) -> None:
                     F[pair[0]][rows, cols, qi] += vals * fac1 * inv_nx
                     F[pair[1]][rows, cols, qi] += vals * fac2 * inv_nx
     st.arrays["F"] = F
+
+
+def crossing_slot(st: State, iq: int, Phi: dict, PhiR: dict) -> dict:
+    """``calculate_PAE`` (parquet_EQOuter.f90:16-118) restricted to the target
+    slot iq (0-based): Phi[r] (Nz, Nz) of that slot, PhiR[r] (Nz*Nz, Nf/2, NR)
+    of all slots, the crossing tensors from ``calc_M``.  Returns F[r] (Nz, Nz)
+    of the slot, the same sums as ``calculate_PAE`` in the same call order."""
+    Nf, Nl, Nz, NR = st.Nf, st.Nl, st.Nz, st.NR
+    aux = abs(1.0 / st.FF[0, 0, 0] * 1.0 / st.FF[0, 0, 0])
+    Om = int(st.ibz[iq, 2])
+    Q = iq // (Nf // 2)
+    F = {r: np.array(Phi[r], dtype=np.complex128, order="F") for r in "dmst"}
+    for r in "dmst":
+        F[r][:Nf, :Nf] += st.L[r][:, :, Om - 1] * aux
+    inv_nx = 1.0 / st.Nx
+    l = np.arange(Nl)
+    nu1 = np.arange(1, Nf + 1)
+    sg = st.signs.astype(np.float64)
+    Mq = {name: st.M_ibz[name][:, :, :, :, Q, :].reshape(Nl * Nl, Nl * Nl * NR, order="F")
+          for name in ("phbar_to_ph", "pp_to_ph", "ph_to_pp", "phbar_to_pp")}
+    for src in "dmst":
+        for w2 in range(1, Nf // 2 + 1):
+            P = PhiR[src][:, w2 - 1, :].reshape(Nz, Nz, NR, order="F")
+            for base, fac1, fac2 in DISPATCH[src]:
+                calls = [base] + ([base + "_TR"] if w2 > 1 else [])
+                for call in calls:
+                    mname, pair, tr = CALLS[call]
+                    valid, t, a, b = crossing_maps(call, w2, np.array([[Om]]), nu1[None, :], Nf)
+                    valid, t, a, b = valid[0], t[0], a[0], b[0]
+                    nv = np.nonzero(valid)[0]
+                    if nv.size == 0:
+                        continue
+                    rows = l[:, None, None] * Nf + (np.clip(a[nv], 1, Nf) - 1)[None, None, :]
+                    cols = l[None, :, None] * Nf + (np.clip(b[nv], 1, Nf) - 1)[None, None, :]
+                    X = P[rows, cols, :]  # (l3, l4, nu, R)
+                    if tr:
+                        X = (sg[:, None] * sg[None, :])[:, :, None, None] * np.conj(X)
+                    Xm = X.transpose(0, 1, 3, 2).reshape(Nl * Nl * NR, nv.size, order="F")
+                    C = (Mq[mname] @ Xm).reshape(Nl, Nl, nv.size, order="F")  # (l1, l2, nu)
+                    ro = l[:, None, None] * Nf + (nu1[nv] - 1)[None, None, :]
+                    co = l[None, :, None] * Nf + (t[nv] - 1)[None, None, :]
+                    ro, co = np.broadcast_arrays(ro, co)
+                    F[pair[0]][ro, co] += C * fac1 * inv_nx
+                    F[pair[1]][ro, co] += C * fac2 * inv_nx
+    return F
 
 
 # --------------------------------------------------------------------------

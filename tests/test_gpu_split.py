@@ -74,10 +74,17 @@ def test_split_bse_against_fp64(gpu_lib):
     sol.close()
 
 
+# Both loops of a fixed-point comparison stop at max|dSigma| < 1e-12, so that
+# the distance of each from the common fixed point (about the last change
+# over one minus the contraction rate) stays well below the 1e-10 bound
+CONV_ABS = 1e-12
+SIGMA_TOL = 1e-10
+
+
 def test_ladder_loop_reaches_the_fp64_fixed_point(gpu_lib):
     from tups_b200 import Params, Solver
     p = Params(beta=3.0, U=2.0, nParticle=0.9, Nx=4, Nf=8, neighbours=2, tprime=-0.1, f_damping=0.5,
-               ite_max=10 ** 6, conv_abs=1e-10)
+               ite_max=10 ** 6, conv_abs=CONV_ABS)
     ref = Solver(p)
     n_ref = 0
     while not ref.iteration(n_ref)["converged"]:
@@ -98,14 +105,14 @@ def test_ladder_loop_reaches_the_fp64_fixed_point(gpu_lib):
         assert n < 3 * n_ref
     # the tuner times FP64 on the first call and tries the split GEMM once
     assert used[0] == 0 and any(u > 0 for u in used)
-    assert parity.rel(sol.Sigma, sig_ref) <= 1e-10 * 50   # 1e-10 absolute on |Sigma| ~ 0.1..1
+    assert parity.rel(sol.Sigma, sig_ref) <= SIGMA_TOL
     sol.close()
 
 
 def test_fixed_slices_loop_reaches_the_fp64_fixed_point(gpu_lib):
     from tups_b200 import Params, Solver
     p = Params(beta=3.0, U=2.0, nParticle=0.9, Nx=4, Nf=8, neighbours=2, tprime=-0.1, f_damping=0.5,
-               ite_max=10 ** 6, conv_abs=1e-10)
+               ite_max=10 ** 6, conv_abs=CONV_ABS)
     sols = {}
     for s in (0, 7):
         sol = Solver(p)
@@ -117,7 +124,7 @@ def test_fixed_slices_loop_reaches_the_fp64_fixed_point(gpu_lib):
         sols[s] = sol.Sigma
         sol.close()
     # 7 slices: GEMM error ~1e-13 relative; the fixed points agree to 1e-10
-    assert parity.rel(sols[7], sols[0]) <= 1e-10
+    assert parity.rel(sols[7], sols[0]) <= SIGMA_TOL
 
 
 def test_graph_iterations_equal_plain_ones(gpu_lib):
@@ -141,7 +148,7 @@ def test_graph_iterations_equal_plain_ones(gpu_lib):
 def test_graph_with_ladder_converges(gpu_lib):
     from tups_b200 import Params, Solver
     p = Params(beta=3.0, U=2.0, nParticle=0.9, Nx=4, Nf=8, neighbours=2, tprime=-0.1, f_damping=0.5,
-               ite_max=10 ** 6, conv_abs=1e-10)
+               ite_max=10 ** 6, conv_abs=CONV_ABS)
     ref = Solver(p)
     n = 0
     while not ref.iteration(n)["converged"]:
@@ -155,5 +162,5 @@ def test_graph_with_ladder_converges(gpu_lib):
     while not sol.iteration(m)["converged"]:
         m += 1
         assert m < 3 * n + 10
-    assert parity.rel(sol.Sigma, sig) <= 1e-10 * 50
+    assert parity.rel(sol.Sigma, sig) <= SIGMA_TOL
     sol.close()

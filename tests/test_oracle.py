@@ -93,6 +93,38 @@ def test_crossing_calls_match_loops():
         assert np.abs(F[r] - st.F[r]).max() <= 1e-13 * np.abs(F[r]).max()
 
 
+@pytest.mark.parametrize("nb", [2, 3])
+def test_slot_restricted_functions_match_the_full_ones(nb):
+    """bse_slot, phir_at_w and crossing_slot (the oracle restricted to single
+    slots, for parity at sizes whose full vertices do not fit the host)
+    against bse / calc_PhiR / calculate_PAE on every channel."""
+    st = O.initialize(small(nb=nb, nf=6))
+    O.iteration(st, 0)
+    O.calc_Gkw_Grt(st, 1, False)
+    G0 = {r: st.G[r].copy() for r in "dmst"}
+    F0 = {r: st.F[r].copy() for r in "dmst"}
+    O.bse(st)
+    slots = [0, st.Nb // 2 + 1, st.Nb - 1]
+    for iq in slots:
+        qx, qy, w = (int(v) for v in st.ibz[iq])
+        cph, cpp = O.calc_chi(st, qx, qy, w)
+        for r in "dmst":
+            got = O.bse_slot(st, r, G0[r][:, :, iq], F0[r][:, :, iq], cph if r in "dm" else cpp)
+            assert np.array_equal(got, st.G[r][:, :, iq])
+    O.calc_PhiR(st)
+    nh, Nz = st.Nf // 2, st.Nz
+    for w in (0, nh - 1):
+        for r in "dmst":
+            PhiQ_w = np.stack([st.G[r][:, :, Q * nh + w].reshape(-1, order="F") for Q in range(st.NIBZ)], axis=1)
+            assert np.array_equal(O.phir_at_w(st, PhiQ_w), st.PhiR[r][:, w, :])
+    Phi = {r: st.G[r].copy() for r in "dmst"}
+    O.calculate_PAE(st)
+    for iq in slots:
+        F = O.crossing_slot(st, iq, {r: Phi[r][:, :, iq] for r in "dmst"}, st.PhiR)
+        for r in "dmst":
+            assert np.abs(F[r] - st.F[r][:, :, iq]).max() <= 1e-14 * np.abs(st.F[r]).max(), (iq, r)
+
+
 def test_sde_and_symop_match_loops():
     st = O.initialize(small(nf=6))
     O.iteration(st, 0)

@@ -87,3 +87,59 @@ def test_bse_noalloc_rejects_oversize(gpu_lib):
     assert rc == -6
     rc = gpu_lib.tups_bse_noalloc(1, 100, 8, 13, dummy, dummy, dummy, 1.0, 0.5, None)
     assert rc == -7
+
+
+def _reference_update(gam, fv, chi, scale, f_damping):
+    """The documented formula, per instance: Phi = scale [(Gamma chi) F +
+    F (chi Gamma)] + (1 - f)(F - Gamma), chi rebuilt dense from its blocks."""
+    n_inst, Nz = gam.shape[0], gam.shape[1]
+    Nl, Nf = chi.shape[1], chi.shape[3]
+    dense = np.zeros((n_inst, Nz, Nz), dtype=np.complex128)
+    nu = np.arange(Nf)
+    for l1 in range(Nl):
+        for l2 in range(Nl):
+            dense[:, l1 * Nf + nu, l2 * Nf + nu] = chi[:, l1, l2, :]
+    gc = np.matmul(gam, dense)
+    cg = np.matmul(dense, gam)
+    return scale * (np.matmul(gc, fv) + np.matmul(fv, cg)) + (1.0 - f_damping) * (fv - gam)
+
+
+@pytest.mark.parametrize("shape", [(576, 9, 64, 8), (1024, 16, 64, 3), (2, 1, 2, 70000)],
+                         ids=["nz576_3_chunks", "nz1024_chunk_1", "nz2_grid_y_cap"])
+def test_bse_noalloc_multiple_chunks(gpu_lib, shape):
+    """More instances than one pass through the static scratch holds: Nz = 576
+    (3 instances per pass), the Nz = 1024 limit (1 per pass) and Nz = 2, where
+    the pass is capped at 65535 instances by the grid; two calls in a row."""
+    import torch
+
+    Nz, Nl, Nf, n_inst = shape
+    rng = np.random.default_rng(Nz + n_inst)
+
+    def crandn(*s):
+        return rng.standard_normal(s) + 1j * rng.standard_normal(s)
+
+    # row-major (inst, col, row) == column-major (row, col) per instance
+    gam = crandn(n_inst, Nz, Nz)
+    fv = crandn(n_inst, Nz, Nz)
+    chi = crandn(n_inst, Nl, Nl, Nf) * 0.1       # (inst, l2, l1, nu) row-major
+    scale, f_damping = 0.37, 0.5
+    # column-major reference: A_cm = X.T per instance
+    chi_cm = np.transpose(chi, (0, 2, 1, 3))       # (inst, l1, l2, nu): chi[l1, l2, nu]
+    ref = _reference_update(np.transpose(gam, (0, 2, 1)), np.transpose(fv, (0, 2, 1)), chi_cm, scale, f_damping)
+    dev = torch.device("cuda:0")
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream(dev)
+    # chi blocks in the documented layout l1 + Nl*(l2 + Nl*nu): row-major (inst, nu, l2, l1)
+    chi_buf = torch.from_numpy(np.ascontiguousarray(np.transpose(chi_cm, (0, 3, 2, 1)))).to(dev)
+    f_buf = torch.from_numpy(fv).to(dev)
+    for call in range(2):
+        g = torch.from_numpy(gam).to(dev)
+        torch.cuda.synchronize(dev)
+        rc = gpu_lib.tups_bse_noalloc(n_inst, Nz, Nf, Nl, C.c_void_p(g.data_ptr()), C.c_void_p(f_buf.data_ptr()),
+                                      C.c_void_p(chi_buf.data_ptr()), scale, f_damping,
+                                      C.c_void_p(stream.cuda_stream))
+        assert rc == 0
+        torch.cuda.synchronize(dev)
+        out = np.transpose(g.cpu().numpy(), (0, 2, 1))
+        err = np.abs(out - ref).max() / np.abs(ref).max()
+        assert err < TOL, (call, err)

@@ -46,14 +46,21 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         return LIB
     build_dir = PKG / "_build"
     build_dir.mkdir(exist_ok=True)
-    objs = []
+    cmds, objs = [], []
     for src in sources():
         obj = build_dir / (src.stem + ".o")
-        cmd = [nvcc(), *ARCH, *FLAGS, "-I", str(INCLUDE), "-c", str(src), "-o", str(obj)]
+        cmds.append([nvcc(), *ARCH, *FLAGS, "-I", str(INCLUDE), "-c", str(src), "-o", str(obj)])
+        objs.append(str(obj))
+    # one nvcc per translation unit, run side by side
+    from concurrent.futures import ThreadPoolExecutor
+
+    def compile_one(cmd):
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
-        objs.append(str(obj))
+
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as pool:
+        list(pool.map(compile_one, cmds))
     tmp = LIB.with_suffix(".so.tmp")
     cmd = [nvcc(), *ARCH, "-shared", "-o", str(tmp), *objs, "-lcudart"]
     subprocess.run(cmd, check=True)

@@ -543,6 +543,32 @@ extern "C" int tups_set_vertex(tups_ctx* ctx, int channel, int which, const doub
   const auto& d = ctx->d;
   return copy_h2d(ctx, p, h, (size_t)d.Nz * d.Nz * d.Nb * sizeof(cplx));
 }
+// a run of `count` consecutive local slots starting at `slot_begin` (0-based)
+static int slot_range(tups_ctx* ctx, int slot_begin, int count, size_t* off, size_t* bytes) {
+  const auto& d = ctx->d;
+  if (slot_begin < 0 || count < 1 || slot_begin > d.Nb - count)
+    return tups::set_error(ctx, TUPS_ERR_BADARG, "slot range outside [0, Nb)");
+  *off = (size_t)d.Nz * d.Nz * slot_begin;
+  *bytes = (size_t)d.Nz * d.Nz * count * sizeof(cplx);
+  return TUPS_OK;
+}
+extern "C" int tups_get_vertex_slots(tups_ctx* ctx, int channel, int which, int slot_begin, int count, double* h) {
+  if (!ctx || !h) return TUPS_ERR_BADARG;
+  cplx* p = vertex_ptr(ctx, channel, which);
+  if (!p) return tups::set_error(ctx, TUPS_ERR_BADARG, "channel/which out of range");
+  size_t off = 0, bytes = 0;
+  TRY(slot_range(ctx, slot_begin, count, &off, &bytes));
+  return copy_d2h(ctx, h, p + off, bytes);
+}
+extern "C" int tups_set_vertex_slots(tups_ctx* ctx, int channel, int which, int slot_begin, int count,
+                                     const double* h) {
+  if (!ctx || !h) return TUPS_ERR_BADARG;
+  cplx* p = vertex_ptr(ctx, channel, which);
+  if (!p) return tups::set_error(ctx, TUPS_ERR_BADARG, "channel/which out of range");
+  size_t off = 0, bytes = 0;
+  TRY(slot_range(ctx, slot_begin, count, &off, &bytes));
+  return copy_h2d(ctx, p + off, h, bytes);
+}
 extern "C" int tups_get_PhiR(tups_ctx* ctx, int channel, double* h) {
   if (!ctx || channel < 0 || channel > 3) return TUPS_ERR_BADARG;
   const auto& d = ctx->d;

@@ -14,10 +14,14 @@
 // exits.  Host code cannot use the array's name as a device address; the
 // address is looked up once per device with cudaGetSymbolAddress (with that
 // device current) on the first call made on the device, so that first call
-// should come before any stream capture.  All calls share the array and it
+// should come before any stream capture.  The address is kept for the life
+// of the process: after a cudaDeviceReset the device's module, and with it
+// the array, is loaded anew, so a process that resets a device must not call
+// this entry point on that device again.  All calls share the array and it
 // keeps the last call's contents; every element a call reads is written by
 // that call first.  Calls whose kernels overlap on the GPU (different
 // streams, or different host threads) race on the array.
+#include <algorithm>
 #include <cstdio>
 #include <mutex>
 
@@ -181,6 +185,9 @@ extern "C" int tups_bse_noalloc(int n_inst, int Nz, int Nf, int Nl, double* gamm
                  Nz, per * sizeof(cplx), kScratchComplex * sizeof(cplx));
     return TUPS_ERR_BADDIM;
   }
+  // an error left by an earlier, unrelated call would otherwise be reported
+  // as this call's launch failure
+  (void)cudaGetLastError();
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) {
     cudaGetLastError();
@@ -190,7 +197,9 @@ extern "C" int tups_bse_noalloc(int n_inst, int Nz, int Nf, int Nl, double* gamm
   int rc = scratch_address(dev, &scratch);
   if (rc != TUPS_OK) return rc;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  const int chunk = (int)(kScratchComplex / per);
+  // instances per pass through the scratch; the instance index is gridDim.y
+  // of both kernels, at most 65535
+  const int chunk = (int)std::min<size_t>(kScratchComplex / per, 65535);
   cplx* A = scratch;
   cplx* B = scratch + (size_t)chunk * Nz * Nz;
   const size_t n2 = (size_t)Nz * Nz;
@@ -200,6 +209,7 @@ extern "C" int tups_bse_noalloc(int n_inst, int Nz, int Nf, int Nl, double* gamm
     dim3 pg((unsigned)(n2 < 256 * 1024 ? (n2 + 255) / 256 : 1024), n);
     k_noalloc_prep<<<pg, 256, 0, st>>>(reinterpret_cast<const cplx*>(gamma_phi), reinterpret_cast<const cplx*>(chi), A,
                                        B, i0, Nz, Nf, Nl);
+    if (cudaGetLastError() != cudaSuccess) return TUPS_ERR_CUDA;
     k_noalloc_gemm<<<dim3(tiles, n), 128, 0, st>>>(reinterpret_cast<cplx*>(gamma_phi), reinterpret_cast<const cplx*>(F),
                                                    A, B, i0, Nz, scale, 1.0 - f_damping);
     if (cudaGetLastError() != cudaSuccess) return TUPS_ERR_CUDA;

@@ -418,6 +418,21 @@ class Solver:
         """G_r array: Gamma_r, or Phi_r between BSE and the vertex update."""
         return self._vertex(channel, 1)
 
+    def vertex_slots(self, channel, which: int, slot_begin: int, count: int = 1) -> np.ndarray:
+        """F_r (which 0) or G_r (which 1) of `count` consecutive local slots
+        from the 0-based `slot_begin`: (Nz, Nz, count)."""
+        ch = CHANNELS.index(channel) if isinstance(channel, str) else int(channel)
+        a = np.empty((self.Nz, self.Nz, count), dtype=np.complex128, order="F")
+        self._call("tups_get_vertex_slots", ch, which, slot_begin, count, _ptr(a))
+        return a
+
+    def set_vertex_slots(self, channel, which: int, slot_begin: int, v: np.ndarray) -> None:
+        ch = CHANNELS.index(channel) if isinstance(channel, str) else int(channel)
+        a = np.asfortranarray(v, dtype=np.complex128)
+        if a.ndim == 2:
+            a = a[:, :, None]
+        self._call("tups_set_vertex_slots", ch, which, slot_begin, a.shape[2], _ptr(a))
+
     def set_vertex(self, channel, which: int, v: np.ndarray) -> None:
         ch = CHANNELS.index(channel) if isinstance(channel, str) else int(channel)
         a = np.asfortranarray(v, dtype=np.complex128)
