@@ -253,6 +253,22 @@ size_t tups_zgemm_split_workspace(int batch, int M, int N, int K, int slices);
 int tups_zgemm_split(int batch, int M, int N, int K, const double* A, const double* B, double* C, int slices,
                      void* work, size_t work_bytes, void* stream);
 
+/* ---- tile-shape tuner -------------------------------------------------------
+ * No counterpart in the reference.  The first FP64 BSE GEMM and the first
+ * crossing call of a context on a new shape time their candidate tilings on
+ * the call's own operands (CUDA events on the library's stream; the BSE on
+ * scratch copies of Gamma) and keep the fastest for that shape in this
+ * process.  The candidates differ only in how output elements are spread over
+ * CTAs and warps, never in the order of a sum, so results do not depend on
+ * the choice.  Not run during a stream capture.  On by default; the
+ * environment variable TUPS_AUTOTUNE=0 or enable = 0 fixes the default tiles. */
+int tups_set_autotune(tups_ctx* ctx, int enable);
+/* The choices made so far in this process as text, one line per kernel and
+ * shape: "<kernel> <shape> | choice <name> | <name>=<ms> ...".  Writes at
+ * most len bytes (NUL-terminated) and returns the length the whole table
+ * needs, NUL included; buf may be NULL with len 0 to ask for it. */
+int tups_get_tuning(char* buf, size_t len);
+
 /* ---- multilayer perceptron of the learned warm start ------------------------
  * No counterpart in the reference.  FP32 network n_in -> n_hidden (x n_layers,
  * SiLU) -> n_out (linear), trained by Adam on the mean squared error.  Flat

@@ -100,6 +100,8 @@ _PROTOS = {
     "tups_set_vertex": [C.c_void_p, C.c_int, C.c_int, C.c_void_p],
     "tups_get_vertex_slots": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p],
     "tups_set_vertex_slots": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p],
+    "tups_set_autotune": [C.c_void_p, C.c_int],
+    "tups_get_tuning": [C.c_char_p, C.c_size_t],
     "tups_get_PhiR": [C.c_void_p, C.c_int, C.c_void_p],
     "tups_get_M": [C.c_void_p, C.c_int, C.c_void_p],
     "tups_get_expSqR": [C.c_void_p, C.c_void_p],

@@ -77,6 +77,7 @@ int bse_async(tups_ctx* ctx, int slices = -1) {
       if (!ctx->tune_ev[i]) TRY(tups::cuda_check(ctx, cudaEventCreate(&ctx->tune_ev[i]), "event"));
     TRY(tups::cuda_check(ctx, cudaEventRecord(ctx->tune_ev[0], ctx->stream), "event"));
   }
+  const long long tunings = ctx->tile_tunings;
   const int chunk_q = (int)std::max<size_t>(1, ctx->s.bse_chunk / 4);
   for (int q0 = 0; q0 < Nb; q0 += chunk_q) {
     const int nq = std::min(chunk_q, Nb - q0);
@@ -85,7 +86,8 @@ int bse_async(tups_ctx* ctx, int slices = -1) {
     tups::phase_end(ctx, TUPS_PHASE_CHI);
     TRY(tups::launch_bse_chunk(ctx, q0, nq));
   }
-  if (tune) {
+  // a call that also timed tile shapes is no measure of the BSE itself
+  if (tune && ctx->tile_tunings == tunings) {
     TRY(tups::cuda_check(ctx, cudaEventRecord(ctx->tune_ev[1], ctx->stream), "event"));
     ctx->tune_pending = ctx->cur_slices;
   }

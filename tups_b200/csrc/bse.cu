@@ -8,6 +8,9 @@
 // GEMM with K = 2 Nz,  [Gamma chi | F] x [F ; chi Gamma],  run on the FP64
 // tensor cores (mma.sync m16n8k8 f64, k_bse_gemm) with the scale and the
 // damping term fused into the epilogue; Phi_r overwrites Gamma_r in place.
+#include <algorithm>
+#include <string>
+
 #include "tups_device.cuh"
 
 namespace tups {
@@ -279,6 +282,58 @@ static int run_gemm(tups_ctx* ctx, const BsePtrs& P, int q_begin, int q_count) {
   return after_launch(ctx, "k_bse_gemm");
 }
 
+// Tile candidates of the FP64 BSE GEMM for Nz >= 32, all with three real
+// products per complex one: they differ in CTA tile, warps and pipeline
+// depth, never in the order of any element's K sum, so every candidate
+// writes the same bits.  Index 0 is the choice measured best on a B200 before
+// the tuner existed: 32 x 32 tiles of 4 warps (16 x 16 each), two cp.async
+// stages (38 KB of shared memory, 5 CTAs per SM): 8x8 / Nl = 5 (Nz = 160)
+// 1.79 ms, against 1.93 ms with three stages, 2.01 ms with BK = 32 and
+// 2.13 ms with four products; 16x16 / Nl = 9 (Nz = 576) 480 ms, against
+// 541 ms for 64 x 64 tiles of 8 warps with four products, 656 ms with three.
+struct BseCand {
+  const char* name;
+  int (*run)(tups_ctx*, const BsePtrs&, int, int);
+};
+static const BseCand kBseCands[] = {
+    {"32x32x16_w2x2_s2", run_gemm<32, 32, 16, 2, 2, 2, true>},
+    {"32x32x16_w2x2_s3", run_gemm<32, 32, 16, 2, 2, 3, true>},
+    {"64x32x16_w4x2_s2", run_gemm<64, 32, 16, 4, 2, 2, true>},
+    {"32x64x16_w2x4_s2", run_gemm<32, 64, 16, 2, 4, 2, true>},
+    {"32x32x32_w2x2_s2", run_gemm<32, 32, 32, 2, 2, 2, true>},
+};
+constexpr int kNumBseCands = sizeof(kBseCands) / sizeof(kBseCands[0]);
+
+// The candidate for this Nz: cached, or timed now on the first chunk's
+// operands (q_begin = 0) with the GEMM writing into scratch copies of the
+// chunk's Gamma, so the call's own result is untouched.
+static int bse_choice(tups_ctx* ctx, const BsePtrs& P, int q_begin, int q_count, int* choice) {
+  const int Nz = ctx->d.Nz;
+  const std::string key = "k_bse_gemm Nz=" + std::to_string(Nz);
+  *choice = 0;
+  if (!ctx->autotune || tune_get(key, choice)) return TUPS_OK;
+  if (q_begin != 0 || !tune_allowed(ctx)) return TUPS_OK;
+  // enough instances for several waves of the smallest tiles
+  const long long tiles32 = (long long)((Nz + 31) / 32) * ((Nz + 31) / 32);
+  const int qt = (int)std::min<long long>(q_count, std::max<long long>(1, (3000 + 4 * tiles32 - 1) / (4 * tiles32)));
+  const size_t n2 = (size_t)Nz * Nz;
+  cplx* scratch = nullptr;
+  int rc = cuda_check(ctx, cudaMalloc(&scratch, 4 * (size_t)qt * n2 * sizeof(cplx)), "tuner scratch");
+  if (rc) return rc;
+  rc = cuda_check(ctx, cudaMemsetAsync(scratch, 0, 4 * (size_t)qt * n2 * sizeof(cplx), ctx->stream), "tuner scratch");
+  BsePtrs T = P;
+  for (int r = 0; r < 4; r++) T.G[r] = scratch + (size_t)r * qt * n2;
+  std::vector<std::string> names;
+  for (int c = 0; c < kNumBseCands; c++) names.push_back(kBseCands[c].name);
+  if (!rc)
+    rc = tune_pick(ctx, key, kNumBseCands, names, [&](int c) { return kBseCands[c].run(ctx, T, 0, qt); }, 2,
+                   choice);
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  cudaFree(scratch);
+  if (!rc && e != cudaSuccess) rc = cuda_check(ctx, e, "tuner");
+  return rc;
+}
+
 // Slices of the split GEMM for the next BSE call; 0 = FP64 tensor cores.
 // Fixed mode: bse_slices.  Ladder: the accuracy needed is chosen from the last
 // relative Sigma change r so that the GEMM error (about 10^(1.1 - 2 s) of
@@ -411,15 +466,13 @@ int launch_bse_chunk(tups_ctx* ctx, int q_begin, int q_count) {
     return rc;
   }
   phase_begin(ctx, TUPS_PHASE_BSE_GEMM);
-  // tile choice, measured on a B200: 32 x 32 tiles of 4 warps (16 x 16 each)
-  // with three real products per complex one on two cp.async stages (38 KB
-  // of shared memory, 5 CTAs per SM by registers) wherever Nz >= 32:
-  // 8x8 / Nl = 5 (Nz = 160) 1.79 ms, against 1.93 ms with three stages,
-  // 2.01 ms with two stages of BK = 32 and 2.13 ms with four products;
-  // 16x16 / Nl = 9 (Nz = 576) 480 ms, against 541 ms for 64 x 64 tiles of
-  // 8 warps (32 x 16 each) with four products and 656 ms with three
-  if (d.Nz >= 32) rc = run_gemm<32, 32, 16, 2, 2, 2, true>(ctx, P, q_begin, q_count);
-  else rc = run_gemm<16, 16, 16, 1, 2, 3, true>(ctx, P, q_begin, q_count);
+  if (d.Nz >= 32) {
+    int choice = 0;
+    rc = bse_choice(ctx, P, q_begin, q_count, &choice);
+    if (!rc) rc = kBseCands[choice].run(ctx, P, q_begin, q_count);
+  } else {
+    rc = run_gemm<16, 16, 16, 1, 2, 3, true>(ctx, P, q_begin, q_count);
+  }
   phase_end(ctx, TUPS_PHASE_BSE_GEMM);
   return rc;
 }

@@ -28,6 +28,8 @@
 // run on the FP64 tensor cores (mma.sync m16n8k8), with X gathered from
 // Phi(R) on load and F = Phi + Lambda*Nc + C/Nx written once in the epilogue:
 // no atomics, deterministic.
+#include <string>
+
 #include "tups_device.cuh"
 
 namespace tups {
@@ -146,6 +148,11 @@ __global__ void k_pae_base(PaePtrs P, const int* __restrict__ ibz, int Nz, int N
 // for one family: C^T[(target, element), (l1,l2)] = X^T[(target, element), (l3,l4,R)] M^T
 // and F_target += C / Nx.  Warps: RW along rows (16 rows each) x WN along
 // the (l1,l2) columns, TN n8 tiles each; BN = 8 TN WN >= Nl^2 (or a chunk).
+// Columns: QN > 0 puts QN IBZ momenta side by side, (momentum, (l1, l2)),
+// one group per blockIdx.x; QN = 0 numbers the columns (momentum, (l1, l2))
+// of all the context's momenta flat and tiles them by BN regardless of
+// momentum boundaries, so only the last tile pads (Nl^2 = 81 at 45 momenta:
+// 3645 columns in 38 tiles of 96, against 45 tiles of 96 with 81 used).
 // The X operand is copied raw: cp.async brings the Phi(R) entries of the two
 // source channels for the K step STG-1 ahead into shared memory, and the
 // dispatch factors, the time-reversal conjugation and its form-factor sign
@@ -178,26 +185,28 @@ __global__ void __launch_bounds__(32 * RW * WN, RW * WN == 8 ? (TN <= 2 ? PAE_MI
   const int pc = blockIdx.y % (2 * nchunks), tile = blockIdx.y / (2 * nchunks);
   const int pair = pc / nchunks, chunk = pc % nchunks;
   // blockIdx.x runs over groups of QN IBZ momenta among those that hold this
-  // context's slots; the group's momenta sit side by side in the columns
-  // (momentum, (l1, l2)), so X serves all of them
+  // context's slots (QN > 0), or over flat column tiles (QN = 0); the
+  // momenta sit side by side in the columns (momentum, (l1, l2)), so X
+  // serves all of them
   const int nh = Nf / 2;
   const int w = blockIdx.z;
+  const int nl2 = Nl * Nl;
   const int Qhi = (slot0 + Nb - 1) / nh;
-  const int Q0 = slot0 / nh + blockIdx.x * QN;
+  const int Q0 = slot0 / nh + (QN > 0 ? blockIdx.x * QN : 0);
+  const int col0 = QN > 0 ? chunk * BN : blockIdx.x * BN;  // first column of the CTA, relative to Q0
   auto local_slot = [&](int iq) {  // local index of slot (Q0 + iq, w), or -1
     const int lq = (Q0 + iq) * nh + w - slot0;
-    return (iq < QN && Q0 + iq <= Qhi && lq >= 0 && lq < Nb) ? lq : -1;
+    return ((QN == 0 || iq < QN) && Q0 + iq <= Qhi && lq >= 0 && lq < Nb) ? lq : -1;
   };
   bool any = false;
-#pragma unroll
-  for (int iq = 0; iq < QN; iq++) any = any || local_slot(iq) >= 0;
+  for (int iq = col0 / nl2; iq <= (col0 + BN - 1) / nl2; iq++) any = any || local_slot(iq) >= 0;
   if (!any) return;
   const int W = ibz[3 * (Q0 * nh + w) + 2];  // the bosonic index of w, the same for every Q
   const int list = pae_list(pair, fam, W, nh);
   const int cnt = counts[list];
   const int e0 = tile * E;
   if (e0 >= cnt) return;
-  const int nl2 = Nl * Nl, nl4 = nl2 * nl2;
+  const int nl4 = nl2 * nl2;
   const int K = nl2 * NR;
   const size_t n2 = (size_t)Nz * Nz;
   const int tid = threadIdx.x;
@@ -257,10 +266,10 @@ __global__ void __launch_bounds__(32 * RW * WN, RW * WN == 8 ? (TN <= 2 ? PAE_MI
     for (int p = tid; p < BN * PAE_BK; p += NT) {
       const int kk = p % PAE_BK, n = p / PAE_BK;
       const int k = kt * PAE_BK + kk;
-      const int nn = chunk * BN + n;
+      const int nn = col0 + n;
       const int iq = QN == 1 ? 0 : nn / nl2;
       const int col = nn - iq * nl2;
-      const bool ok = k < K && col < nl2 && iq < QN && Q0 + iq <= Qhi;
+      const bool ok = k < K && col < nl2 && (QN == 0 || iq < QN) && Q0 + iq <= Qhi;
       const cplx* src = Mf;
       if (ok) {
         const int l34 = k % nl2, R = k / nl2;
@@ -343,7 +352,7 @@ __global__ void __launch_bounds__(32 * RW * WN, RW * WN == 8 ? (TN <= 2 ? PAE_MI
 #pragma unroll
     for (int x = 0; x < 4; x++) {
       const int e = er + (x >= 2 ? 8 : 0);
-      const int nn = chunk * BN + (wc * TN + j) * 8 + 2 * tig + (x & 1);
+      const int nn = col0 + (wc * TN + j) * 8 + 2 * tig + (x & 1);
       const int iq = QN == 1 ? 0 : nn / nl2;
       const int col = nn - iq * nl2;
       if (col >= nl2 || e0 + e >= cnt) continue;
@@ -377,7 +386,9 @@ static int run_pae(tups_ctx* ctx, const PaePtrs& P, int nchunks, int fam, int ma
   if (max_tiles == 0) return TUPS_OK;
   const int nh = d.Nf / 2;
   const int nQ = (ctx->slot0 + d.Nb - 1) / nh - ctx->slot0 / nh + 1;  // momenta holding this context's slots
-  dim3 grid((nQ + QN - 1) / QN, max_tiles * 2 * nchunks, nh);
+  const int gx = QN > 0 ? (nQ + QN - 1) / QN : (nQ * d.Nl * d.Nl + BN - 1) / BN;
+  if (QN == 0) nchunks = 1;
+  dim3 grid(gx, max_tiles * 2 * nchunks, nh);
   kern<<<grid, 32 * RW * WN, sm, ctx->stream>>>(P, ctx->t.pae_elems, ctx->t.pae_counts, ctx->t.ibz, ctx->t.signs,
                                                 d.Nz, d.Nf, d.Nl, d.NIBZ, d.NR, nchunks, fam, Kpad, ctx->slot0,
                                                 d.Nb, 1.0 / d.Nx);
@@ -424,6 +435,52 @@ static int build_pae_lists(tups_ctx* ctx) {
   return cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "PAE lists");
 }
 
+// Tile candidates of the crossing kernel per form-factor count.  They differ
+// in how the (target, element) rows and the (momentum, (l1, l2)) columns are
+// spread over CTAs and warps; every output element is still summed over K in
+// the same order, so all candidates write the same bits.  Index 0 is the
+// default when the tuner is off.  Measured on a B200 before the tuner: at
+// Nl^2 = 25 three momenta side by side (75 of 80 columns used) 1.76 ms at
+// 8x8 / Nl = 5 against 1.89 ms with one momentum per CTA; at Nl^2 = 81 one
+// momentum per 96-column CTA, two CTAs per SM, 482 ms at 16x16 / Nl = 9
+// (one 16-warp CTA of 64 elements per SM 540 ms, 64 elements x 48 columns in
+// two chunks 491 ms).
+struct PaeCand {
+  const char* name;
+  int (*run)(tups_ctx*, const PaePtrs&, int, int, int);
+  int bn;  // columns per CTA; chunks of BN per momentum when QN = 1
+};
+static const PaeCand kPaeNl1[] = {
+    {"flat_bn8_tn1", run_pae<1, 1, 4, 2, 0>, 8},
+    {"flat_bn16_tn2", run_pae<2, 1, 4, 2, 0>, 16},
+    {"q1_bn8_tn1", run_pae<1, 1, 4, 2, 1>, 8},
+};
+static const PaeCand kPaeNl5[] = {
+    {"q3_bn80_tn5", run_pae<5, 2, 4, 2, 3>, 80},
+    {"flat_bn80_tn5", run_pae<5, 2, 4, 2, 0>, 80},
+    {"flat_bn64_tn4", run_pae<4, 2, 4, 2, 0>, 64},
+    {"flat_bn48_tn3", run_pae<3, 2, 4, 2, 0>, 48},
+};
+static const PaeCand kPaeWide[] = {
+    {"flat_bn96_tn6", run_pae<6, 2, 4, 2, 0>, 96},
+    {"q1_bn96_tn6", run_pae<6, 2, 4, 2, 1>, 96},
+    {"flat_bn80_tn5", run_pae<5, 2, 4, 2, 0>, 80},
+    {"flat_bn64_tn4", run_pae<4, 2, 4, 2, 0>, 64},
+    {"flat_bn112_tn7", run_pae<7, 2, 4, 2, 0>, 112},
+};
+
+static int pae_all(tups_ctx* ctx, const PaePtrs& P, const PaeCand& c) {
+  const auto& d = ctx->d;
+  const size_t n = (size_t)d.Nz * d.Nz * d.Nb;
+  dim3 bgrid((unsigned)std::min<size_t>(cdiv(n, 256), 148 * 8), 4);
+  k_pae_base<<<bgrid, 256, 0, ctx->stream>>>(P, ibz_local(ctx), d.Nz, d.Nf, d.Nb,
+                                             std::fabs(1.0 / ctx->FF[0] * 1.0 / ctx->FF[0]));
+  int rc = after_launch(ctx, "k_pae_base");
+  const int nchunks = (d.Nl * d.Nl + c.bn - 1) / c.bn;
+  for (int fam = 0; fam < 2 && !rc; fam++) rc = c.run(ctx, P, nchunks, fam, ctx->pae_max_tiles[fam]);
+  return rc;
+}
+
 int launch_pae(tups_ctx* ctx) {
   const auto& d = ctx->d;
   if (d.Nl > 13) return set_error(ctx, TUPS_ERR_BADDIM, "Nl > 13 not supported by the crossing kernel");
@@ -441,27 +498,24 @@ int launch_pae(tups_ctx* ctx) {
     P.F[r] = ctx->s.F[r];
   }
   // F = Phi + Lambda Nc, then the diagonal family, then the anti-diagonal one
-  const size_t n = (size_t)d.Nz * d.Nz * d.Nb;
-  dim3 bgrid((unsigned)std::min<size_t>(cdiv(n, 256), 148 * 8), 4);
-  k_pae_base<<<bgrid, 256, 0, ctx->stream>>>(P, ibz_local(ctx), d.Nz, d.Nf, d.Nb, std::fabs(1.0 / ctx->FF[0] * 1.0 / ctx->FF[0]));
-  int rc = after_launch(ctx, "k_pae_base");
-  if (rc) return rc;
   const int nl2 = d.Nl * d.Nl;
-  for (int fam = 0; fam < 2; fam++) {
-    const int mc = ctx->pae_max_tiles[fam];
-    // tile configs measured on a B200: 8 warps x 32 elements throughout; at
-    // Nl^2 = 81, 96 columns with two CTAs per SM (16x16 / Nl = 9: 482 ms; one
-    // 16-warp CTA of 64 elements per SM 540 ms, 64 elements x 48 columns in
-    // two chunks 491 ms)
-    if (nl2 <= 8) rc = run_pae<1, 1, 4, 2>(ctx, P, 1, fam, mc);
-    // Nl^2 = 25: three IBZ momenta side by side in the columns, 75 of 80
-    // used instead of 25 of 32 (8x8 / Nl = 5: 1.76 ms against 1.89 ms)
-    else if (3 * nl2 <= 80) rc = run_pae<5, 2, 4, 2, 3>(ctx, P, 1, fam, mc);
-    else if (nl2 <= 32) rc = run_pae<2, 2, 4, 2>(ctx, P, 1, fam, mc);
-    else rc = run_pae<6, 2, 4, 2>(ctx, P, (nl2 + 95) / 96, fam, mc);
+  const PaeCand* cands = nl2 <= 8 ? kPaeNl1 : nl2 <= 32 ? kPaeNl5 : kPaeWide;
+  const int n_cand = nl2 <= 8 ? (int)(sizeof(kPaeNl1) / sizeof(PaeCand))
+                     : nl2 <= 32 ? (int)(sizeof(kPaeNl5) / sizeof(PaeCand))
+                                 : (int)(sizeof(kPaeWide) / sizeof(PaeCand));
+  const std::string key = "k_pae_mma Nl=" + std::to_string(d.Nl) + " Nf=" + std::to_string(d.Nf) +
+                          " NIBZ=" + std::to_string(d.NIBZ) + " NR=" + std::to_string(d.NR) +
+                          " Nb=" + std::to_string(d.Nb) + " slot0=" + std::to_string(ctx->slot0);
+  int choice = 0;
+  if (ctx->autotune && !tune_get(key, &choice) && tune_allowed(ctx)) {
+    std::vector<std::string> names;
+    for (int c = 0; c < n_cand; c++) names.push_back(cands[c].name);
+    // every run rebuilds F from Phi, so timing the candidates in place is
+    // harmless; the chosen one runs last
+    int rc = tune_pick(ctx, key, n_cand, names, [&](int c) { return pae_all(ctx, P, cands[c]); }, 2, &choice);
     if (rc) return rc;
   }
-  return TUPS_OK;
+  return pae_all(ctx, P, cands[choice]);
 }
 
 }  // namespace tups

@@ -4,6 +4,7 @@
 #include <cctype>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <sstream>
@@ -790,6 +791,10 @@ static int ctx_create(const tups_params* p, int device, int rank, int ntasks, tu
   tups_ctx* ctx = new tups_ctx();
   ctx->p = *p;
   ctx->device = device;
+  {
+    const char* at = std::getenv("TUPS_AUTOTUNE");
+    if (at && at[0] == '0') ctx->autotune = false;
+  }
   int rc = build_tables(ctx);
   if (rc == TUPS_OK) rc = shard_slots(ctx, rank, ntasks);
   if (rc == TUPS_OK) rc = tups::cuda_check(ctx, cudaSetDevice(device), "cudaSetDevice");

@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstring>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -146,6 +148,10 @@ struct tups_ctx {
   // in graph mode the tuner compares whole-iteration times (tune_graph_ms)
   bool use_graph = false;
   bool capturing = false;
+  // tile-shape tuner (tune.cu): on by default, TUPS_AUTOTUNE=0 turns it off;
+  // tile_tunings counts the tunings run by this context
+  bool autotune = true;
+  long long tile_tunings = 0;
   cudaGraphExec_t graph_exec[18] = {};
   long long graph_launches[18] = {};
   double tune_graph_ms[9] = {-1, -1, -1, -1, -1, -1, -1, -1, -1};
@@ -215,6 +221,15 @@ void oz_bind_work(OzRun& R, const OzWork& w, void* base);
 int oz_run(OzRun& R, cudaStream_t stream, long long* launches);
 
 int set_error(tups_ctx* ctx, int code, const std::string& msg);
+
+// tile-shape tuner, tune.cu: process-wide choices keyed by kernel and shape
+bool tune_get(const std::string& key, int* choice);
+// false when the context has tuning off or its stream is being captured
+bool tune_allowed(tups_ctx* ctx);
+// time run(c) for c = 0..n_cand-1 (best of reps, CUDA events on the
+// context's stream), store and return the fastest in *choice
+int tune_pick(tups_ctx* ctx, const std::string& key, int n_cand, const std::vector<std::string>& names,
+              const std::function<int(int)>& run, int reps, int* choice);
 // sharded contexts: combine n doubles at device address dev over the ranks
 // (no-op unsharded); synchronises the stream first
 int exchange(tups_ctx* ctx, int what, double* dev, size_t n, int op);

@@ -288,6 +288,10 @@ class Solver:
         """Replay iterations (from ite 1 on) from captured CUDA graphs."""
         self._call("tups_set_graph", int(bool(enable)))
 
+    def set_autotune(self, enable: bool = True) -> None:
+        """Tile-shape tuner on (default) or off (fixed default tiles)."""
+        self._call("tups_set_autotune", int(bool(enable)))
+
     # -- split-precision BSE --
     def set_bse_precision(self, slices: int = 0, ladder: bool = False) -> None:
         """slices = 0: FP64 tensor cores; 2..8: int8 slices per operand;
@@ -517,3 +521,13 @@ def _conv_dict(ci: tups_conv_info) -> dict:
         d[f"F_{r}_max"] = ci.F_max[i]
         d[f"rel_err_{r}"] = ci.rel_err[i]
     return d
+
+
+def tuning_table() -> list[str]:
+    """The tile-shape tuner's choices in this process, one line per kernel
+    and shape: ``key | choice NAME | NAME=ms ...``."""
+    lib = _lib.load()
+    n = lib.tups_get_tuning(None, 0)
+    buf = C.create_string_buffer(max(1, n))
+    lib.tups_get_tuning(buf, len(buf))
+    return [ln for ln in buf.value.decode().splitlines() if ln]
