@@ -261,6 +261,7 @@ def run_tups(args, wl_name: str, wl: dict):
     torch.cuda.set_device(device)
     ranks = replicas.init("nccl")
     from tups_b200 import Params, Solver, load
+    from tups_b200.parquet import tuning_table
     load()
     peak64 = fp64_peak_tflops(device)
     params = Params(**{k: v for k, v in wl.items() if k in Params.__dataclass_fields__})
@@ -390,6 +391,7 @@ def run_tups(args, wl_name: str, wl: dict):
                     "api": "Solver.set_sigma_from(pinned) + Solver.iteration + Solver.get_sigma_into(pinned)"},
             "gpu_launches": launches,
             "clocks": clk,
+            "tuning": tuning_table(),
             "cpu_baseline": cpu,
             "last_conv": {k: infos[-1][k] for k in ("rel_sig_max", "dsigma_inf", "mu")} if infos else None,
         }
@@ -475,30 +477,34 @@ def _rel(a, b) -> float:
     return float(np.max(np.abs(a - b))) / den if den > 0 else float(np.max(np.abs(a - b)))
 
 
-def to_convergence(params, device: int, max_iter: int = 3000, graph: bool = True) -> dict:
+def to_convergence(params, device: int, conv_abs: float = 1e-10, ref_abs: float = 1e-13, max_iter: int = 3000,
+                   graph: bool = True) -> dict:
     """Wall time (device events around the host-driven loop) and iterations to
-    max|dSigma| < 1e-10 from the reference's initial state: FP64 BSE vs the
-    precision ladder, both replaying CUDA graphs.  Then the converged states
-    against each other, max-norm relative error per quantity: Sigma, F_r and
-    Gamma_r of each channel, the chi0 bubble and the susceptibilities sus_r
-    of the readout (the FP64 path equals the oracle to 1e-12 per phase)."""
+    max|dSigma| < conv_abs from the reference's initial state: FP64 BSE vs the
+    precision ladder, both replaying CUDA graphs.  Then the converged states,
+    max-norm relative error per quantity (Sigma, F_r and Gamma_r of each
+    channel, the chi0 bubble and the susceptibilities sus_r of the readout):
+    the ladder's against the FP64 loop's, and both against the fixed point
+    itself, the FP64 loop continued (untimed) to max|dSigma| < ref_abs.  The
+    FP64 path equals the oracle to 1e-12 per phase."""
     from dataclasses import replace
     from tups_b200 import Solver
-    p = replace(params, conv_abs=1e-10, ite_max=10 ** 6)
-    res = {}
+    p = replace(params, conv_abs=conv_abs, ite_max=10 ** 6)
+    res = {"conv_abs": conv_abs}
     fin = {}
     for name in ("fp64", "ladder"):
         sol = Solver(p, device=device)
         sol.set_graph(graph)
         if name == "ladder":
             sol.set_bse_precision(0, ladder=True)
-        used = []
+        used, dsig = [], []
         sol.synchronize()
         sol.record_event(4)
         n, ok = 0, False
         while n < max_iter:
             used.append(sol.bse_slices)
             ci = sol.iteration(n)
+            dsig.append(ci["dsigma_inf"])
             n += 1
             if ci["converged"]:
                 ok = True
@@ -508,16 +514,30 @@ def to_convergence(params, device: int, max_iter: int = 3000, graph: bool = True
         full = sol.Nz * sol.Nz * sol.Nb * 16 * 8 < 4e9
         slots = [0, sol.Nb // 2, sol.Nb - 1]
         fin[name] = _final_state(sol, n, full, slots)
-        sol.close()
         res[name] = {"iterations": n, "seconds": sec, "s_per_iter": sec / n, "converged": ok}
         if name == "ladder":
             res[name]["slices_per_iteration"] = used
-    a, b = fin["ladder"], fin["fp64"]
-    errs = {k: _rel(a[k], b[k]) for k in b}
+        else:
+            # contraction rate of the loop near its fixed point
+            tail = [d for d in dsig[-20:] if d > 0]
+            if len(tail) >= 2:
+                res[name]["contraction_rate"] = float((tail[-1] / tail[0]) ** (1.0 / (len(tail) - 1)))
+            m = n + 1
+            while m < max_iter:
+                ci = sol.iteration(m)
+                m += 1
+                if ci["dsigma_inf"] < ref_abs:
+                    break
+            fin["fixed"] = _final_state(sol, m, full, slots)
+            res["fixed_point"] = {"max_dsigma": ref_abs, "iterations": m + 1,
+                                  "note": "the FP64 loop continued past its stop, untimed"}
+        sol.close()
+    errs = {k: _rel(fin["ladder"][k], fin["fp64"][k]) for k in fin["fp64"]}
     res["rel_err_ladder_vs_fp64"] = errs
-    res["rel_err_note"] = ("max-norm relative difference of the ladder's converged state from the FP64 one, "
-                           "both stopped at max|dSigma| < 1e-10; vertices " +
-                           ("whole" if full else "at slots [0, Nb/2, Nb-1]") +
+    res["rel_err_vs_fixed_point"] = {name: {k: _rel(fin[name][k], fin["fixed"][k]) for k in fin["fixed"]}
+                                     for name in ("fp64", "ladder")}
+    res["rel_err_note"] = ("max-norm relative differences of converged states, both loops stopped at max|dSigma| < "
+                           f"{conv_abs:g}; vertices " + ("whole" if full else "at slots [0, Nb/2, Nb-1]") +
                            "; Gamma_r after the vertex update; chi0/sus from the readout of one more iteration")
     res["sigma_rel_err_ladder_vs_fp64"] = errs["Sigma"]
     res["speedup_ladder_vs_fp64"] = res["fp64"]["seconds"] / res["ladder"]["seconds"]
@@ -530,8 +550,8 @@ TARGET_WORKLOAD = "pa_16x16_nl9_nf64"
 
 def target_record(device: int) -> dict:
     """The 16x16 k / 9 form factor / 64 frequency loop (t' = -0.2, n = 0.85,
-    U = 3, beta = 10): FP64 vs precision-ladder time to max|dSigma| < 1e-10
-    and the converged states' difference, with its own clock samples.  The
+    U = 3, beta = 10): FP64 vs precision-ladder time to max|dSigma| < 1e-11
+    and the converged states' errors, with its own clock samples.  The
     learned warm start is trained on the 8x8 / 5 form-factor grid and has no
     network for this grid, so the ladder runs from the cold start."""
     from tups_b200 import Params
@@ -540,7 +560,9 @@ def target_record(device: int) -> dict:
     clocks = ClockSampler(device)
     clocks.start()
     t0 = time.perf_counter()
-    conv = to_convergence(params, device)
+    # max|dSigma| < 1e-11: with the loop's contraction rate near 0.87 both
+    # runs then stop within about 1e-10 of the fixed point in Sigma
+    conv = to_convergence(params, device, conv_abs=1e-11)
     wall = time.perf_counter() - t0
     clk = clocks.stop()
     return {"workload": TARGET_WORKLOAD,
@@ -551,6 +573,7 @@ def target_record(device: int) -> dict:
 
 
 LU_WORKLOAD = "bse_lu_1024"
+SPLIT_LU_SLICES = (3, 4, 5, 6)
 
 
 def run_bse_batched(args):
@@ -627,6 +650,23 @@ def run_bse_batched(args):
     e3.record(stream)
     torch.cuda.synchronize(device)
     ms_e2e = e2.elapsed_time(e3) / K
+    split = {}
+    for sl in SPLIT_LU_SLICES:
+        info = batch.run_split(slices=sl, tol=1e-12, max_refine=8)
+        torch.cuda.synchronize(device)
+        s0 = torch.cuda.Event(enable_timing=True)
+        s1 = torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        for _ in range(K):
+            batch.run_split(slices=sl, tol=1e-12, max_refine=8, check=False)
+        s1.record(stream)
+        torch.cuda.synchronize(device)
+        ms_s = s0.elapsed_time(s1) / K
+        res_s = batch.results()
+        err_s = max(float(np.abs(res_s[i] - ref[i]).max() / np.abs(ref[i]).max()) for i in sample)
+        split[str(sl)] = {"ms": ms_s, "effective_tflops": flops / (ms_s * 1e-3) / 1e12, "speedup_vs_fp64_lu": ms / ms_s,
+                          "max_rel_err_vs_lapack": err_s, "refinements": int(info["refinements"].max()),
+                          "max_correction": float(info["correction"].max())}
     line = {"metric": "BSE TFLOP/s", "value": tf, "unit": "TFLOP/s", "n_gpus": ws, "steps": K, "warmup": W,
             "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "config": cfg,
@@ -634,6 +674,10 @@ def run_bse_batched(args):
                          "unit": "TFLOP/s", "frac": tf / peak64, "traffic": None,
                          "peak_source": "FP64 cuBLAS ZGEMM 4096^3 measured in this run"},
             "max_rel_err_vs_lapack": err,
+            "split_precision_refined": split,
+            "split_note": ("tups_bse_lu_split_batched: LU and solve updates on s int8 slices (tcgen05), FP64 residual "
+                           "and refinement to max|correction| <= 1e-12 max|F|; effective TFLOP/s = the FP64 LU's "
+                           "algorithmic (8/3 + 8) n^3 / time"),
             "e2e": {"value": flops / (ms_e2e * 1e-3) / 1e12, "unit": "TFLOP/s",
                     "h2d_bytes_per_step": int(hg.numel() * 16 + hc.numel() * 16),
                     "d2h_bytes_per_step": int(ho.numel() * 16)},

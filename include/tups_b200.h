@@ -359,6 +359,29 @@ int tups_bse_lu_batched(int n_inst, const int* n, const int* nl, const double* s
                         const double* chi, double* out, double* work, int* ipiv, int want_phi, int* status,
                         void* stream);
 
+/* ---- LU form in split precision with FP64 iterative refinement ---------------
+ * No counterpart in the reference (see tups_bse_lu_batched).  The same
+ * F_i = (1 - scale_i Gamma_i chi_i)^{-1} Gamma_i (want_phi: F_i - Gamma_i)
+ * with the arithmetic split: instances grouped by size; blocked LU with
+ * partial pivoting whose 128-column panels are factored in FP64 and whose
+ * trailing updates, like the off-diagonal updates of the triangular solves,
+ * run on the int8 tensor cores with `slices` (2..8) int8 slices per operand
+ * (error about 10^(1.1 - 2 slices) of the update's norm); then iterative
+ * refinement with the residual Gamma - A X in FP64 (FP64 tensor cores),
+ * X += U^{-1} L^{-1} P residual, until max|correction| <= tol max|X| for
+ * every instance of a size group or max_refine steps.  refinements and
+ * correction (host, optional, n_inst entries): steps taken and the last
+ * relative correction of each instance (-1 with max_refine = 0); status as in
+ * tups_bse_lu_batched.  work: device buffer of tups_bse_lu_split_workspace()
+ * bytes (the largest size group's five n x n matrices per instance, pivots and
+ * the split-GEMM slices).  Synchronises the stream once per refinement step;
+ * TUPS_ERR_TIMEOUT when a bounded wait of the int8 GEMM ran out. */
+size_t tups_bse_lu_split_workspace(int n_inst, const int* n, int slices);
+int tups_bse_lu_split_batched(int n_inst, const int* n, const int* nl, const double* scale, const double* gamma,
+                              const double* chi, double* out, int want_phi, int slices, double tol, int max_refine,
+                              void* work, size_t work_bytes, int* refinements, double* correction, int* status,
+                              void* stream);
+
 /* ---- BSE update without device allocation ----------------------------------
  * No counterpart in the reference.  For callers that may not allocate device
  * memory while they call this library (a host that gives all device memory

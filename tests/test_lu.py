@@ -70,3 +70,39 @@ def test_batched_lu_reports_singular_pivot(gpu_lib):
                      gamma=[g], chi=[chi], q=np.zeros((1, 3), dtype=np.int32))
     with pytest.raises(TupsError, match="singular"):
         solve(inst)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("slices", [4, 5, 7])
+def test_split_lu_with_refinement_matches_lapack(gpu_lib, slices):
+    """Split-precision LU (int8 trailing and solve updates) refined in FP64
+    to the LAPACK answer; sizes up to 2 blocks of 128 plus a ragged tail."""
+    from tups_b200.bse_batched import make_instances, solve_split
+    inst = make_instances(n_q=4, n_w=4, nf=48, seed=13, nff_choices=(1, 5, 9))  # n in {48, 240, 432}
+    assert len(set(inst.n.tolist())) >= 2
+    F, info = solve_split(inst, slices=slices, tol=1e-12, max_refine=8)
+    assert np.all(info["correction"] <= 1e-12), info
+    for i, (g, c) in enumerate(zip(inst.gamma, inst.chi)):
+        ref = LU.bse_lu(g, c, 1.0)
+        err = np.abs(F[i] - ref).max() / np.abs(ref).max()
+        assert err < 1e-12, (i, int(inst.n[i]), slices, err)
+    # fewer slices need more refinement steps, never fewer
+    assert int(info["refinements"].max()) >= 1
+
+
+@pytest.mark.gpu
+def test_split_lu_phi_scale_and_unrefined_error(gpu_lib):
+    """want_phi and per-instance scales; without refinement the error is the
+    split GEMM's, after refinement the FP64 LU's."""
+    from tups_b200.bse_batched import LuBatch, make_instances
+    inst = make_instances(n_q=2, n_w=3, nf=40, seed=5, rho=0.5, nff_choices=(1, 5))
+    inst.scale = np.linspace(0.5, 1.5, len(inst.n))
+    b = LuBatch(inst)
+    refs = [LU.bse_lu(g, c, float(inst.scale[i])) - g for i, (g, c) in enumerate(zip(inst.gamma, inst.chi))]
+    errs = {}
+    for steps in (0, 8):
+        info = b.run_split(slices=3, tol=1e-13, max_refine=steps, want_phi=True)
+        out = b.results()
+        errs[steps] = max(np.abs(out[i] - refs[i]).max() / np.abs(refs[i]).max() for i in range(len(refs)))
+    assert 1e-9 < errs[0] < 1e-2, errs
+    assert errs[8] < 1e-12, errs

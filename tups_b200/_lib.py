@@ -101,6 +101,10 @@ _PROTOS = {
     "tups_get_vertex_slots": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p],
     "tups_set_vertex_slots": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p],
     "tups_set_autotune": [C.c_void_p, C.c_int],
+    "tups_bse_lu_split_batched": [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double),
+                                  C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_int,
+                                  C.c_void_p, C.c_size_t, C.POINTER(C.c_int), C.POINTER(C.c_double),
+                                  C.POINTER(C.c_int), C.c_void_p],
     "tups_get_tuning": [C.c_char_p, C.c_size_t],
     "tups_get_PhiR": [C.c_void_p, C.c_int, C.c_void_p],
     "tups_get_M": [C.c_void_p, C.c_int, C.c_void_p],
@@ -140,6 +144,7 @@ _SPECIAL = {
     "tups_mlp_last_error": ([C.c_void_p], C.c_char_p),
     "tups_get_bse_slices": ([C.c_void_p], C.c_int),
     "tups_zgemm_split_workspace": ([C.c_int, C.c_int, C.c_int, C.c_int, C.c_int], C.c_size_t),
+    "tups_bse_lu_split_workspace": ([C.c_int, C.POINTER(C.c_int), C.c_int], C.c_size_t),
     "tups_mlp_num_params": ([C.c_void_p], C.c_longlong),
     "tups_mlp_kernel_launches": ([C.c_void_p], C.c_longlong),
 }

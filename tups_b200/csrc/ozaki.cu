@@ -319,7 +319,7 @@ __device__ __forceinline__ uint64_t oz_desc(uint32_t saddr) {
 // buffer into FP64 registers, acc += 2^(-7(d+2)) D_d, while the MMAs of the
 // next diagonals proceed; after the last diagonal they apply the row and
 // column scales and the epilogue, and the next tile starts.
-enum { OZ_EPI_ZGEMM = 0, OZ_EPI_BSE = 1 };
+enum { OZ_EPI_ZGEMM = 0, OZ_EPI_BSE = 1, OZ_EPI_SUB = 2 };
 
 constexpr int OZ_NBUF = 4;            // TMEM accumulator buffers
 constexpr int OZ_MAX_NT = 128;        // columns per tile
@@ -338,7 +338,9 @@ struct OzGemm {
   double* status;        // set to status_code on a timed-out wait
   double status_code;
   int epi;
-  cplx* C;               // OZ_EPI_ZGEMM: col-major M x N per instance
+  cplx* C;               // OZ_EPI_ZGEMM: col-major M x N per instance; OZ_EPI_SUB: C -= A B
+  int ldc;               // OZ_EPI_SUB: leading dimension and instance stride of C
+  long long c_stride;
   cplx* F[4];            // OZ_EPI_BSE: Phi = scale[r] C + omf (F - G) over G
   cplx* G[4];
   double scale[4];
@@ -523,6 +525,8 @@ __global__ void __launch_bounds__(OZ_THREADS2, 1)
         r = inst % 4;
         Fq = P.F[r] + (size_t)P.M * P.M * q;
         Gq = P.G[r] + (size_t)P.M * P.M * q;
+      } else if (P.epi == OZ_EPI_SUB) {
+        Cq = P.C + (size_t)inst * P.c_stride;
       } else {
         Cq = P.C + (size_t)inst * P.M * P.N;
       }
@@ -533,6 +537,12 @@ __global__ void __launch_bounds__(OZ_THREADS2, 1)
           const int jc = np >> 1;
           const double sc = rs * P.cscale[(size_t)inst * P.N + jc];
           const double cre = acc[c] * sc, cim = acc[c + 1] * sc;
+          if (P.epi == OZ_EPI_SUB) {
+            const size_t ix = m + (size_t)P.ldc * jc;
+            const cplx c0 = Cq[ix];
+            Cq[ix] = cmk(c0.x - cre, c0.y - cim);
+            continue;
+          }
           const size_t idx = m + (size_t)P.M * jc;
           if (P.epi == OZ_EPI_ZGEMM) {
             Cq[idx] = cmk(cre, cim);
@@ -686,6 +696,8 @@ int oz_run(OzRun& R, cudaStream_t stream, long long* launches) {
   P.status_code = R.status_code;
   P.epi = R.epi;
   P.C = R.C;
+  P.ldc = R.ldc;
+  P.c_stride = R.c_stride;
   for (int r = 0; r < 4; r++) {
     P.F[r] = R.F[r];
     P.G[r] = R.G[r];

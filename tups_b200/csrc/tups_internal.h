@@ -206,8 +206,10 @@ struct OzRun {
   double* acc = nullptr;
   double* status = nullptr;   // receives status_code when a wait times out
   double status_code = 0.0;
-  int epi = 0;         // 0: C = A B; 1: BSE update written over G
+  int epi = 0;         // 0: C = A B; 1: BSE update written over G; 2: C -= A B
   cplx* C = nullptr;
+  int ldc = 0;              // epi 2: leading dimension of C and the complex
+  long long c_stride = 0;   // stride between instances
   cplx* F[4] = {};
   cplx* G[4] = {};
   double scale[4] = {};
