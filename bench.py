@@ -312,6 +312,15 @@ def run_tups(args, wl_name: str, wl: dict):
         sol.iteration(W + 2 * K + k)
     phases = sol.phase_times()
     sol.set_timing(False)
+    readout_ms = None
+    if args.with_readout:
+        # one output iteration with the chi readout (off the timed path)
+        ite = W + 2 * K
+        ite += (5 - ite % 5) % 5
+        sol.record_event(6)
+        sol.iteration(ite, readout=True)
+        sol.record_event(7)
+        readout_ms = sol.event_elapsed_ms(6, 7)
     # ---- max over ranks ----
     ms, ms_e2e = replicas.max_over_ranks(ranks, [ms, ms_e2e])
     value = replicas.seconds_per_iteration(ms, K, ws)
@@ -392,6 +401,7 @@ def run_tups(args, wl_name: str, wl: dict):
             "gpu_launches": launches,
             "clocks": clk,
             "tuning": tuning_table(),
+            "readout_iteration_ms": readout_ms,
             "cpu_baseline": cpu,
             "last_conv": {k: infos[-1][k] for k in ("rel_sig_max", "dsigma_inf", "mu")} if infos else None,
         }
@@ -574,6 +584,7 @@ def target_record(device: int) -> dict:
 
 LU_WORKLOAD = "bse_lu_1024"
 SPLIT_LU_SLICES = (3, 4, 5, 6)
+SPLIT_LU_TOL = 1e-12
 
 
 def run_bse_batched(args):
@@ -652,13 +663,13 @@ def run_bse_batched(args):
     ms_e2e = e2.elapsed_time(e3) / K
     split = {}
     for sl in SPLIT_LU_SLICES:
-        info = batch.run_split(slices=sl, tol=1e-12, max_refine=8)
+        info = batch.run_split(slices=sl, tol=SPLIT_LU_TOL, max_refine=8)
         torch.cuda.synchronize(device)
         s0 = torch.cuda.Event(enable_timing=True)
         s1 = torch.cuda.Event(enable_timing=True)
         s0.record(stream)
         for _ in range(K):
-            batch.run_split(slices=sl, tol=1e-12, max_refine=8, check=False)
+            batch.run_split(slices=sl, tol=SPLIT_LU_TOL, max_refine=8, check=False)
         s1.record(stream)
         torch.cuda.synchronize(device)
         ms_s = s0.elapsed_time(s1) / K
@@ -666,7 +677,7 @@ def run_bse_batched(args):
         err_s = max(float(np.abs(res_s[i] - ref[i]).max() / np.abs(ref[i]).max()) for i in sample)
         split[str(sl)] = {"ms": ms_s, "effective_tflops": flops / (ms_s * 1e-3) / 1e12, "speedup_vs_fp64_lu": ms / ms_s,
                           "max_rel_err_vs_lapack": err_s, "refinements": int(info["refinements"].max()),
-                          "max_correction": float(info["correction"].max())}
+                          "max_rel_residual": float(info["residual"].max())}
     line = {"metric": "BSE TFLOP/s", "value": tf, "unit": "TFLOP/s", "n_gpus": ws, "steps": K, "warmup": W,
             "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "config": cfg,
@@ -676,8 +687,8 @@ def run_bse_batched(args):
             "max_rel_err_vs_lapack": err,
             "split_precision_refined": split,
             "split_note": ("tups_bse_lu_split_batched: LU and solve updates on s int8 slices (tcgen05), FP64 residual "
-                           "and refinement to max|correction| <= 1e-12 max|F|; effective TFLOP/s = the FP64 LU's "
-                           "algorithmic (8/3 + 8) n^3 / time"),
+                           "Gamma - A F, corrections until max|residual| <= 1e-12 max|Gamma|; effective TFLOP/s = "
+                           "the FP64 LU's algorithmic (8/3 + 8) n^3 / time"),
             "e2e": {"value": flops / (ms_e2e * 1e-3) / 1e12, "unit": "TFLOP/s",
                     "h2d_bytes_per_step": int(hg.numel() * 16 + hc.numel() * 16),
                     "d2h_bytes_per_step": int(ho.numel() * 16)},
@@ -686,13 +697,91 @@ def run_bse_batched(args):
         print(json.dumps(line), flush=True)
 
 
+ZGEMM_WORKLOAD = "zgemm_split"
+
+
+def run_zgemm_split(args):
+    """Throughput of the split-precision batched ZGEMM (tups_zgemm_split)
+    against cuBLAS ZGEMM at the BSE GEMM's shape: batched C_b = A_b B_b with
+    M = N = Nz and K = 2 Nz ([Gamma chi | F] [F ; chi Gamma] for
+    Nz = Nl * Nf).  Seeded random complex128 inputs, device-resident; CUDA
+    events on the launching stream after one untimed call.  One JSON line with
+    a record per slice count: effective FP64-equivalent TFLOP/s (8 M N K per
+    entry), int8 tensor rate and the error against the FP64 product."""
+    import ctypes as C
+    import torch
+    from tups_b200 import load
+    ws_, rank, local = dist_env()
+    if rank != 0:
+        return
+    lib = load()
+    torch.cuda.set_device(local)
+    Nz, batch, reps = args.nz, args.batch, max(1, args.steps)
+    M = N = Nz
+    K = 2 * Nz
+    g = torch.Generator(device="cuda")
+    g.manual_seed(1234)
+    A = torch.randn((batch, K, M), dtype=torch.complex128, device="cuda", generator=g)
+    B = torch.randn((batch, N, K), dtype=torch.complex128, device="cuda", generator=g)
+    Cm = torch.zeros((batch, N, M), dtype=torch.complex128, device="cuda")
+    stream = torch.cuda.current_stream()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    At, Bt = A.transpose(1, 2), B.transpose(1, 2)
+    ref = torch.matmul(At[:1], Bt[:1])[0]
+
+    def time_cublas() -> float:
+        for _ in range(3):
+            torch.matmul(At, Bt)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(reps):
+            torch.matmul(At, Bt)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    zgemm_ms = time_cublas()
+    flops = 8.0 * M * N * K * batch
+    out = {}
+    for s in args.slices:
+        wsz = lib.tups_zgemm_split_workspace(batch, M, N, K, s)
+        work = torch.empty(wsz, dtype=torch.uint8, device="cuda")
+        cargs = (batch, M, N, K, C.c_void_p(A.data_ptr()), C.c_void_p(B.data_ptr()), C.c_void_p(Cm.data_ptr()), s,
+                 C.c_void_p(work.data_ptr()), wsz, C.c_void_p(stream.cuda_stream))
+        rc = lib.tups_zgemm_split(*cargs)
+        if rc:
+            raise RuntimeError(f"tups_zgemm_split failed with {rc}")
+        err = float((Cm[0].transpose(0, 1) - ref).abs().max() / ref.abs().max())
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(reps):
+            lib.tups_zgemm_split(*cargs)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        pairs = s * (s + 1) // 2
+        out[str(s)] = {"ms": ms, "effective_tflops": flops / ms / 1e9,
+                       "int8_tops": 2.0 * pairs * M * (2 * N) * (2 * K) * batch / ms / 1e9,
+                       "rel_err_vs_fp64": err}
+        del work
+    zgemm_ms = min(zgemm_ms, time_cublas())
+    line = {"metric": "split ZGEMM effective TFLOP/s", "unit": "TFLOP/s", "workload": ZGEMM_WORKLOAD,
+            "config": {"Nz": Nz, "batch": batch, "M": M, "N": N, "K": K}, "steps": reps,
+            "cublas_zgemm_ms": zgemm_ms, "cublas_zgemm_tflops": flops / zgemm_ms / 1e9, "slices": out}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["tups", "reference"], default="tups")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + [LU_WORKLOAD], default=DEFAULT_WORKLOAD)
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + [LU_WORKLOAD, ZGEMM_WORKLOAD], default=DEFAULT_WORKLOAD)
+    ap.add_argument("--nz", type=int, default=576, help="zgemm_split: M = N = Nz, K = 2 Nz")
+    ap.add_argument("--batch", type=int, default=64, help="zgemm_split: batch entries")
+    ap.add_argument("--slices", type=int, nargs="+", default=[2, 3, 4, 5, 6, 7, 8], help="zgemm_split: slice counts")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-split", action="store_true", help="skip the split-precision iterations")
     ap.add_argument("--no-graph", action="store_true", help="launch the timed iterations kernel by kernel")
@@ -701,6 +790,8 @@ def main():
     ap.add_argument("--no-convergence", action="store_true", help="skip the runs to convergence")
     ap.add_argument("--convergence", action="store_true",
                     help="also run the loops to convergence when Nz > 256 (minutes at 16x16)")
+    ap.add_argument("--with-readout", action="store_true",
+                    help="after the timed region, one output iteration with the chi readout")
     ap.add_argument("--no-target", action="store_true",
                     help="skip the 16x16 / 9 form factor FP64-vs-ladder record (about 6 minutes)")
     args = ap.parse_args()
@@ -708,6 +799,12 @@ def main():
         args.warmup = 3
     if args.workload == LU_WORKLOAD:
         run_bse_batched(args)
+        return
+    if args.workload == ZGEMM_WORKLOAD:
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the split ZGEMM has no CPU counterpart"}))
+            return
+        run_zgemm_split(args)
         return
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":

@@ -252,6 +252,16 @@ int tups_get_bse_slices(const tups_ctx* ctx);
 size_t tups_zgemm_split_workspace(int batch, int M, int N, int K, int slices);
 int tups_zgemm_split(int batch, int M, int N, int K, const double* A, const double* B, double* C, int slices,
                      void* work, size_t work_bytes, void* stream);
+/* Failure detection of the split GEMM's bounded device waits (its pipeline
+ * barriers).  cycles > 0: a wait of the work loop gives up after that many SM
+ * clock cycles (0 restores the default, about 2 s); the CTA then waits for
+ * its copies and MMAs already in flight, frees its tensor memory and returns,
+ * and the call (or the next conv/iteration of a context) reports
+ * TUPS_ERR_TIMEOUT.  stall_test = 1: the next split GEMM launch first waits
+ * on a barrier that nothing signals, so that wait runs out (a test of the
+ * timeout path that faults nothing); later launches run normally.
+ * Process-wide. */
+int tups_set_split_wait(long long cycles, int stall_test);
 
 /* ---- tile-shape tuner -------------------------------------------------------
  * No counterpart in the reference.  The first FP64 BSE GEMM and the first
@@ -367,19 +377,18 @@ int tups_bse_lu_batched(int n_inst, const int* n, const int* nl, const double* s
  * trailing updates, like the off-diagonal updates of the triangular solves,
  * run on the int8 tensor cores with `slices` (2..8) int8 slices per operand
  * (error about 10^(1.1 - 2 slices) of the update's norm); then iterative
- * refinement with the residual Gamma - A X in FP64 (FP64 tensor cores),
- * X += U^{-1} L^{-1} P residual, until max|correction| <= tol max|X| for
- * every instance of a size group or max_refine steps.  refinements and
- * correction (host, optional, n_inst entries): steps taken and the last
- * relative correction of each instance (-1 with max_refine = 0); status as in
- * tups_bse_lu_batched.  work: device buffer of tups_bse_lu_split_workspace()
+ * refinement: the residual R = Gamma - A X in FP64 (FP64 tensor cores) and,
+ * until max|R| <= tol max|Gamma| for every instance of a size group or after
+ * max_refine corrections, X += U^{-1} L^{-1} P R.  refinements and residual
+ * (host, optional, n_inst entries): corrections applied and the final
+ * max|R|/max|Gamma| of each instance; status as in tups_bse_lu_batched.  work: device buffer of tups_bse_lu_split_workspace()
  * bytes (the largest size group's five n x n matrices per instance, pivots and
  * the split-GEMM slices).  Synchronises the stream once per refinement step;
  * TUPS_ERR_TIMEOUT when a bounded wait of the int8 GEMM ran out. */
 size_t tups_bse_lu_split_workspace(int n_inst, const int* n, int slices);
 int tups_bse_lu_split_batched(int n_inst, const int* n, const int* nl, const double* scale, const double* gamma,
                               const double* chi, double* out, int want_phi, int slices, double tol, int max_refine,
-                              void* work, size_t work_bytes, int* refinements, double* correction, int* status,
+                              void* work, size_t work_bytes, int* refinements, double* residual, int* status,
                               void* stream);
 
 /* ---- BSE update without device allocation ----------------------------------

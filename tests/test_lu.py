@@ -81,12 +81,12 @@ def test_split_lu_with_refinement_matches_lapack(gpu_lib, slices):
     inst = make_instances(n_q=4, n_w=4, nf=48, seed=13, nff_choices=(1, 5, 9))  # n in {48, 240, 432}
     assert len(set(inst.n.tolist())) >= 2
     F, info = solve_split(inst, slices=slices, tol=1e-12, max_refine=8)
-    assert np.all(info["correction"] <= 1e-12), info
+    assert np.all(info["residual"] <= 1e-12), info
     for i, (g, c) in enumerate(zip(inst.gamma, inst.chi)):
         ref = LU.bse_lu(g, c, 1.0)
         err = np.abs(F[i] - ref).max() / np.abs(ref).max()
         assert err < 1e-12, (i, int(inst.n[i]), slices, err)
-    # fewer slices need more refinement steps, never fewer
+    # the int8 factors alone are not FP64-accurate: at least one correction
     assert int(info["refinements"].max()) >= 1
 
 
@@ -101,7 +101,7 @@ def test_split_lu_phi_scale_and_unrefined_error(gpu_lib):
     refs = [LU.bse_lu(g, c, float(inst.scale[i])) - g for i, (g, c) in enumerate(zip(inst.gamma, inst.chi))]
     errs = {}
     for steps in (0, 8):
-        info = b.run_split(slices=3, tol=1e-13, max_refine=steps, want_phi=True)
+        info = b.run_split(slices=3, tol=1e-12, max_refine=steps, want_phi=True)
         out = b.results()
         errs[steps] = max(np.abs(out[i] - refs[i]).max() / np.abs(refs[i]).max() for i in range(len(refs)))
     assert 1e-9 < errs[0] < 1e-2, errs

@@ -203,9 +203,9 @@ class LuBatch:
                   check: bool = True) -> dict:
         """The same solve in split precision with FP64 iterative refinement
         (``tups_bse_lu_split_batched``): LU and triangular-solve updates on
-        int8 slices (tcgen05), residual Gamma - A X in FP64, refinement
-        until max|correction| <= tol max|X| per instance.  Returns the
-        refinement steps and final relative corrections per instance."""
+        int8 slices (tcgen05), residual Gamma - A X in FP64, corrections
+        until max|residual| <= tol max|Gamma| per instance.  Returns the
+        corrections applied and the final relative residual per instance."""
         import torch
         nI = len(self.n)
         nptr = self.n.ctypes.data_as(C.POINTER(C.c_int))
@@ -215,20 +215,20 @@ class LuBatch:
         if getattr(self, "split_work", None) is None or self.split_work.numel() < need:
             self.split_work = torch.empty(need, dtype=torch.uint8, device=self.dev)
         steps = np.zeros(nI, dtype=np.int32)
-        corr = np.zeros(nI, dtype=np.float64)
+        resid = np.zeros(nI, dtype=np.float64)
         stream = torch.cuda.current_stream(self.dev)
         rc = self.lib.tups_bse_lu_split_batched(
             nI, nptr, self.nl.ctypes.data_as(C.POINTER(C.c_int)), self.sc.ctypes.data_as(C.POINTER(C.c_double)),
             C.c_void_p(self.dg.data_ptr()), C.c_void_p(self.dc.data_ptr()), C.c_void_p(self.out.data_ptr()),
             int(want_phi), int(slices), float(tol), int(max_refine), C.c_void_p(self.split_work.data_ptr()),
             C.c_size_t(self.split_work.numel()), steps.ctypes.data_as(C.POINTER(C.c_int)),
-            corr.ctypes.data_as(C.POINTER(C.c_double)), self.status.ctypes.data_as(C.POINTER(C.c_int)),
+            resid.ctypes.data_as(C.POINTER(C.c_double)), self.status.ctypes.data_as(C.POINTER(C.c_int)),
             C.c_void_p(stream.cuda_stream))
         if rc != 0:
             raise TupsError(rc, "tups_bse_lu_split_batched failed")
         if check and np.any(self.status):
             raise TupsError(-4, f"singular pivot in instances {np.nonzero(self.status)[0].tolist()}")
-        return {"refinements": steps, "correction": corr}
+        return {"refinements": steps, "residual": resid}
 
     def results(self) -> list:
         host = self.out.cpu().numpy()

@@ -17,10 +17,11 @@
 //    of 32 plus FP64 tensor-core updates), the off-diagonal updates on the
 //    int8 path.
 //  * Refinement: R = Gamma - A X = Gamma - X + c Gamma (chi X) in FP64 (the
-//    GEMM on the FP64 tensor cores, three real products per complex one),
-//    D = U^{-1} L^{-1} P R as above, X += D, until max|D| <= tol max|X| for
-//    every instance of the group or max_refine steps.  Each step multiplies
-//    the error by about kappa(A) 10^(1.1-2s).
+//    GEMM on the FP64 tensor cores, three real products per complex one);
+//    stop when max|R| <= tol max|Gamma| for every instance of the group (or
+//    after max_refine corrections), else D = U^{-1} L^{-1} P R as above and
+//    X += D.  Each correction multiplies the error by about
+//    kappa(A) 10^(1.1-2s).
 //
 // Caller-owned workspace only (tups_bse_lu_split_workspace bytes).
 #include <algorithm>
@@ -71,13 +72,15 @@ __device__ double block_max(double v) {
 // FP64 LU form in lu.cu)
 __global__ void __launch_bounds__(LS_THREADS) k_ls_form(const LsDesc* __restrict__ desc, const cplx* __restrict__ gamma,
                                                         const cplx* __restrict__ chi_all, cplx* __restrict__ Gg,
-                                                        cplx* __restrict__ Xg, cplx* __restrict__ Ag, int n) {
+                                                        cplx* __restrict__ Xg, cplx* __restrict__ Ag,
+                                                        unsigned long long* gmax, int n) {
   const int i = blockIdx.y;
   const LsDesc d = desc[i];
   const int nl = d.nl, nf = n / nl;
   const size_t n2 = (size_t)n * n;
   const cplx* G = gamma + d.g_off;
   const cplx* chi = chi_all + d.c_off;
+  double mx = 0.0;
   for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n2; e += (size_t)gridDim.x * blockDim.x) {
     const int row = (int)(e % n), col = (int)(e / n);
     const int l2 = col / nf, nu = col % nf;
@@ -87,37 +90,56 @@ __global__ void __launch_bounds__(LS_THREADS) k_ls_form(const LsDesc* __restrict
     Gg[n2 * i + e] = g;
     Xg[n2 * i + e] = g;
     Ag[n2 * i + e] = cmk((row == col ? 1.0 : 0.0) - d.scale * acc.x, -d.scale * acc.y);
+    mx = fmax(mx, fmax(fabs(g.x), fabs(g.y)));
   }
+  mx = block_max(mx);
+  if (threadIdx.x == 0) atomic_max_nonneg(&gmax[i], mx);
 }
 
-// B[0:kb, 0:ncols] = L^{-1} B, L unit lower kb x kb; one thread per column
-__device__ void trsm_unit_lower(const cplx* L, cplx* B, int kb, int ncols, int ldl, int ldb) {
-  for (int col = threadIdx.x; col < ncols; col += blockDim.x) {
-    cplx* b = B + (size_t)ldb * col;
-    for (int r = 1; r < kb; r++) {
-      cplx acc = b[r];
-      for (int k = 0; k < r; k++) acc = csub(acc, cmul(L[r + (size_t)ldl * k], b[k]));
-      b[r] = acc;
+// one column b[0:kb] = L^{-1} b (L unit lower, kb <= 32) with the column in
+// registers: b[r] -= L[r, k] b[k] for k < r in ascending order
+__device__ __forceinline__ void col_lower(const cplx* __restrict__ L, int ldl, cplx* b, int kb) {
+  cplx v[LS_SUB];
+#pragma unroll
+  for (int r = 0; r < LS_SUB; r++) v[r] = r < kb ? b[r] : cmk(0.0, 0.0);
+#pragma unroll
+  for (int r = 1; r < LS_SUB; r++) {
+    if (r < kb) {
+      cplx acc = v[r];
+#pragma unroll
+      for (int k = 0; k < r; k++) acc = csub(acc, cmul(L[r + (size_t)ldl * k], v[k]));
+      v[r] = acc;
     }
   }
+#pragma unroll
+  for (int r = 0; r < LS_SUB; r++)
+    if (r < kb) b[r] = v[r];
 }
 
-// B[0:kb, 0:ncols] = U^{-1} B, U upper kb x kb with its diagonal
-__device__ void trsm_upper(const cplx* U, cplx* B, int kb, int ncols, int ldu, int ldb) {
-  for (int col = threadIdx.x; col < ncols; col += blockDim.x) {
-    cplx* b = B + (size_t)ldb * col;
-    for (int r = kb - 1; r >= 0; r--) {
-      cplx acc = b[r];
-      for (int k = r + 1; k < kb; k++) acc = csub(acc, cmul(U[r + (size_t)ldu * k], b[k]));
+// one column b[0:kb] = U^{-1} b (U upper with its diagonal, kb <= 32)
+__device__ __forceinline__ void col_upper(const cplx* __restrict__ U, int ldu, cplx* b, int kb) {
+  cplx v[LS_SUB];
+#pragma unroll
+  for (int r = 0; r < LS_SUB; r++) v[r] = r < kb ? b[r] : cmk(0.0, 0.0);
+#pragma unroll
+  for (int r = LS_SUB - 1; r >= 0; r--) {
+    if (r < kb) {
+      cplx acc = v[r];
+#pragma unroll
+      for (int k = r + 1; k < LS_SUB; k++)
+        if (k < kb) acc = csub(acc, cmul(U[r + (size_t)ldu * k], v[k]));
       const cplx u = U[r + (size_t)ldu * r];
-      b[r] = (u.x == 0.0 && u.y == 0.0) ? acc : cmul(acc, crecip(u));
+      v[r] = (u.x == 0.0 && u.y == 0.0) ? acc : cmul(acc, crecip(u));
     }
   }
+#pragma unroll
+  for (int r = 0; r < LS_SUB; r++)
+    if (r < kb) b[r] = v[r];
 }
 
 // Panel [j0, j0 + jb) of every instance of the group (one CTA each): partial
-// pivoting LU of rows j0..n-1 in sub-panels of 32, the panel's row
-// interchanges on all other columns, and U12 = L11^{-1} A12.
+// pivoting LU of rows j0..n-1 in sub-panels of 32, within the panel's columns
+// (k_ls_rows applies its interchanges to the other columns and forms U12).
 __global__ void __launch_bounds__(LS_THREADS) k_ls_panel(cplx* __restrict__ Ag, int* __restrict__ ipiv_all,
                                                          int* __restrict__ status, int n, int j0, int jb) {
   __shared__ double s_val[LS_THREADS / 32];
@@ -204,37 +226,53 @@ __global__ void __launch_bounds__(LS_THREADS) k_ls_panel(cplx* __restrict__ Ag, 
     }
     const int rc = je - jj - kb;
     if (rc > 0) {
-      trsm_unit_lower(A + jj + (size_t)n * jj, A + jj + (size_t)n * (jj + kb), kb, rc, n, n);
+      for (int col = tid; col < rc; col += nt)
+        col_lower(A + jj + (size_t)n * jj, n, A + jj + (size_t)n * (jj + kb + col), kb);
       __syncthreads();
       rank_update(A + (jj + kb) + (size_t)n * (jj + kb), A + (jj + kb) + (size_t)n * jj, A + jj + (size_t)n * (jj + kb),
                   n - jj - kb, rc, kb, n, n, n);
       __syncthreads();
     }
   }
-  // the panel's interchanges on the columns outside it
-  for (int c = j0; c < je; c++) {
-    const int p = ipiv[c];
-    if (p != c)
-      for (int col = tid; col < n; col += nt) {
-        if (col >= j0 && col < je) continue;
-        const cplx t = A[c + (size_t)n * col];
-        A[c + (size_t)n * col] = A[p + (size_t)n * col];
-        A[p + (size_t)n * col] = t;
+}
+
+// Columns outside the panel [j0, j0 + jb), LS_COLS per CTA (grid (column
+// chunks, instances)): the panel's row interchanges, thread per column, then
+// for the columns right of the panel U12 = L11^{-1} A12 in sub-blocks of 32
+// (column in registers) with the FP64 tensor-core update between them.
+constexpr int LS_COLS = 128;
+
+__global__ void __launch_bounds__(LS_COLS) k_ls_rows(cplx* __restrict__ Ag, const int* __restrict__ ipiv_all, int n,
+                                                     int j0, int jb) {
+  const int i = blockIdx.y;
+  cplx* A = Ag + (size_t)n * n * i;
+  const int* ipiv = ipiv_all + (size_t)n * i;
+  const int je = j0 + jb;
+  const int c0 = blockIdx.x * LS_COLS;
+  const int col = c0 + threadIdx.x;
+  if (col < n && (col < j0 || col >= je)) {
+    cplx* x = A + (size_t)n * col;
+    for (int c = j0; c < je; c++) {
+      const int p = ipiv[c];
+      if (p != c) {
+        const cplx t = x[c];
+        x[c] = x[p];
+        x[p] = t;
       }
+    }
+  }
+  const int ca = max(c0, je), cb = min(c0 + LS_COLS, n);  // this CTA's columns of A12
+  if (ca >= cb) return;
+  __syncthreads();
+  for (int jj = j0; jj < je; jj += LS_SUB) {
+    const int kb = min(LS_SUB, je - jj);
+    if (col >= ca && col < cb) col_lower(A + jj + (size_t)n * jj, n, A + jj + (size_t)n * col, kb);
+    __syncthreads();
+    if (jj + kb < je)
+      rank_update(A + (jj + kb) + (size_t)n * ca, A + (jj + kb) + (size_t)n * jj, A + jj + (size_t)n * ca,
+                  je - jj - kb, cb - ca, kb, n, n, n);
     __syncthreads();
   }
-  // U12 = L11^{-1} A12, blocked by 32
-  const int ncols = n - je;
-  if (ncols > 0)
-    for (int jj = j0; jj < je; jj += LS_SUB) {
-      const int kb = min(LS_SUB, je - jj);
-      trsm_unit_lower(A + jj + (size_t)n * jj, A + jj + (size_t)n * je, kb, ncols, n, n);
-      __syncthreads();
-      if (jj + kb < je)
-        rank_update(A + (jj + kb) + (size_t)n * je, A + (jj + kb) + (size_t)n * jj, A + jj + (size_t)n * je,
-                    je - jj - kb, ncols, kb, n, n, n);
-      __syncthreads();
-    }
 }
 
 // X <- P X: every thread applies the whole interchange sequence to its columns
@@ -255,34 +293,44 @@ __global__ void __launch_bounds__(LS_THREADS) k_ls_perm(cplx* __restrict__ Xg, c
   }
 }
 
-// forward substitution on the diagonal block [j0, j0 + jb) (unit lower), all n columns
-__global__ void __launch_bounds__(LS_THREADS) k_ls_fwd_diag(const cplx* __restrict__ Ag, cplx* __restrict__ Xg, int n,
-                                                            int j0, int jb) {
-  const int i = blockIdx.x;
+// forward substitution on the diagonal block [j0, j0 + jb) (unit lower),
+// LS_COLS columns of the right-hand sides per CTA
+__global__ void __launch_bounds__(LS_COLS) k_ls_fwd_diag(const cplx* __restrict__ Ag, cplx* __restrict__ Xg, int n,
+                                                         int j0, int jb) {
+  const int i = blockIdx.y;
   const cplx* A = Ag + (size_t)n * n * i;
   cplx* X = Xg + (size_t)n * n * i;
   const int je = j0 + jb;
+  const int ca = blockIdx.x * LS_COLS, cb = min(ca + LS_COLS, n);
+  const int col = ca + threadIdx.x;
   for (int jj = j0; jj < je; jj += LS_SUB) {
     const int kb = min(LS_SUB, je - jj);
-    trsm_unit_lower(A + jj + (size_t)n * jj, X + jj, kb, n, n, n);
+    if (col < cb) col_lower(A + jj + (size_t)n * jj, n, X + jj + (size_t)n * col, kb);
     __syncthreads();
-    if (jj + kb < je) rank_update(X + (jj + kb), A + (jj + kb) + (size_t)n * jj, X + jj, je - jj - kb, n, kb, n, n, n);
+    if (jj + kb < je)
+      rank_update(X + (jj + kb) + (size_t)n * ca, A + (jj + kb) + (size_t)n * jj, X + jj + (size_t)n * ca,
+                  je - jj - kb, cb - ca, kb, n, n, n);
     __syncthreads();
   }
 }
 
-// back substitution on the diagonal block [j0, j0 + jb) (upper), all n columns
-__global__ void __launch_bounds__(LS_THREADS) k_ls_bwd_diag(const cplx* __restrict__ Ag, cplx* __restrict__ Xg, int n,
-                                                            int j0, int jb) {
-  const int i = blockIdx.x;
+// back substitution on the diagonal block [j0, j0 + jb) (upper), LS_COLS
+// columns per CTA
+__global__ void __launch_bounds__(LS_COLS) k_ls_bwd_diag(const cplx* __restrict__ Ag, cplx* __restrict__ Xg, int n,
+                                                         int j0, int jb) {
+  const int i = blockIdx.y;
   const cplx* A = Ag + (size_t)n * n * i;
   cplx* X = Xg + (size_t)n * n * i;
+  const int ca = blockIdx.x * LS_COLS, cb = min(ca + LS_COLS, n);
+  const int col = ca + threadIdx.x;
   const int nsub = (jb + LS_SUB - 1) / LS_SUB;
   for (int t = nsub - 1; t >= 0; t--) {
     const int jj = j0 + t * LS_SUB, kb = min(LS_SUB, j0 + jb - jj);
-    trsm_upper(A + jj + (size_t)n * jj, X + jj, kb, n, n, n);
+    if (col < cb) col_upper(A + jj + (size_t)n * jj, n, X + jj + (size_t)n * col, kb);
     __syncthreads();
-    if (jj > j0) rank_update(X + j0, A + j0 + (size_t)n * jj, X + jj, jj - j0, n, kb, n, n, n);
+    if (jj > j0)
+      rank_update(X + j0 + (size_t)n * ca, A + j0 + (size_t)n * jj, X + jj + (size_t)n * ca, jj - j0, cb - ca, kb, n,
+                  n, n);
     __syncthreads();
   }
 }
@@ -318,7 +366,7 @@ constexpr int RS_BM = 32, RS_BN = 32, RS_BK = 16, RS_LDL = RS_BM + 2, RS_LDR = R
 
 __global__ void __launch_bounds__(128) k_ls_resid(const LsDesc* __restrict__ desc, const cplx* __restrict__ Gg,
                                                   const cplx* __restrict__ Yg, const cplx* __restrict__ Xg,
-                                                  cplx* __restrict__ Rg, int n) {
+                                                  cplx* __restrict__ Rg, unsigned long long* rmax, int n) {
   __shared__ __align__(16) cplx sL[2][RS_BK][RS_LDL];
   __shared__ __align__(16) cplx sR[2][RS_BN][RS_LDR];
   const int i = blockIdx.y;
@@ -373,6 +421,7 @@ __global__ void __launch_bounds__(128) k_ls_resid(const LsDesc* __restrict__ des
   const double s = desc[i].scale;
   const cplx* Xi = Xg + n2 * i;
   cplx* Ri = Rg + n2 * i;
+  double mx = 0.0;
 #pragma unroll
   for (int j = 0; j < 2; j++)
 #pragma unroll
@@ -382,31 +431,21 @@ __global__ void __launch_bounds__(128) k_ls_resid(const LsDesc* __restrict__ des
         const size_t idx = row + (size_t)n * col;
         const double cre = p1[j][x] - p2[j][x], cim = p3[j][x] - p1[j][x] - p2[j][x];
         const cplx g = Gi[idx], xv = Xi[idx];
-        Ri[idx] = cmk((g.x - xv.x) + s * cre, (g.y - xv.y) + s * cim);
+        const cplx rv = cmk((g.x - xv.x) + s * cre, (g.y - xv.y) + s * cim);
+        Ri[idx] = rv;
+        mx = fmax(mx, fmax(fabs(rv.x), fabs(rv.y)));
       }
     }
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if (lane == 0) atomic_max_nonneg(&rmax[i], mx);
 }
 
-// X += D; dmax[i] = max|D_i|, xmax[i] = max|X_i| (componentwise max norm)
-__global__ void __launch_bounds__(LS_THREADS) k_ls_update(cplx* __restrict__ Xg, const cplx* __restrict__ Dg,
-                                                          unsigned long long* dmax, unsigned long long* xmax, int n) {
+// X += D
+__global__ void __launch_bounds__(LS_THREADS) k_ls_update(cplx* __restrict__ Xg, const cplx* __restrict__ Dg, int n) {
   const int i = blockIdx.y;
   const size_t n2 = (size_t)n * n;
-  double md = 0.0, mx = 0.0;
-  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n2; e += (size_t)gridDim.x * blockDim.x) {
-    const cplx dv = Dg[n2 * i + e];
-    cplx xv = Xg[n2 * i + e];
-    xv = cadd(xv, dv);
-    Xg[n2 * i + e] = xv;
-    md = fmax(md, fmax(fabs(dv.x), fabs(dv.y)));
-    mx = fmax(mx, fmax(fabs(xv.x), fabs(xv.y)));
-  }
-  md = block_max(md);
-  mx = block_max(mx);
-  if (threadIdx.x == 0) {
-    atomic_max_nonneg(&dmax[i], md);
-    atomic_max_nonneg(&xmax[i], mx);
-  }
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n2; e += (size_t)gridDim.x * blockDim.x)
+    Xg[n2 * i + e] = cadd(Xg[n2 * i + e], Dg[n2 * i + e]);
 }
 
 // out_i = X_i (want_phi: X_i - Gamma_i) at the instance's place in the caller's layout
@@ -435,7 +474,7 @@ LsLayout ls_layout(int b, int n, int slices) {
   L.mat = up256((size_t)b * n * n * sizeof(cplx));
   L.ipiv = up256((size_t)b * n * sizeof(int));
   L.desc = up256((size_t)b * sizeof(LsDesc));
-  L.norms = up256((size_t)2 * b * sizeof(unsigned long long));
+  L.norms = up256((size_t)2 * b * sizeof(unsigned long long));  // max|R_i|, max|Gamma_i|
   L.status = up256((size_t)b * sizeof(int) + sizeof(double));
   L.oz = up256(oz_work_layout(b, n, n, std::min(LS_NB, n), slices).total + 256);
   L.total = 5 * L.mat + L.ipiv + L.desc + L.norms + L.status + L.oz + 256;
@@ -482,7 +521,7 @@ int ls_solve(cudaStream_t st, cplx* Ag, cplx* Xg, const int* ipiv, void* ozw, in
   (*launches)++;
   for (int j0 = 0; j0 < n; j0 += LS_NB) {
     const int jb = std::min(LS_NB, n - j0), je = j0 + jb;
-    k_ls_fwd_diag<<<b, LS_THREADS, 0, st>>>(Ag, Xg, n, j0, jb);
+    k_ls_fwd_diag<<<dim3((n + LS_COLS - 1) / LS_COLS, b), LS_COLS, 0, st>>>(Ag, Xg, n, j0, jb);
     (*launches)++;
     if (je < n) {
       int rc = ls_gemm_sub(st, ozw, b, n - je, n, jb, Ag + je + (size_t)n * j0, n, Xg + j0, n, Xg + je, n, n2, s,
@@ -493,7 +532,7 @@ int ls_solve(cudaStream_t st, cplx* Ag, cplx* Xg, const int* ipiv, void* ozw, in
   const int nblk = (n + LS_NB - 1) / LS_NB;
   for (int bk = nblk - 1; bk >= 0; bk--) {
     const int j0 = bk * LS_NB, jb = std::min(LS_NB, n - j0);
-    k_ls_bwd_diag<<<b, LS_THREADS, 0, st>>>(Ag, Xg, n, j0, jb);
+    k_ls_bwd_diag<<<dim3((n + LS_COLS - 1) / LS_COLS, b), LS_COLS, 0, st>>>(Ag, Xg, n, j0, jb);
     (*launches)++;
     if (j0 > 0) {
       int rc = ls_gemm_sub(st, ozw, b, j0, n, jb, Ag + (size_t)n * j0, n, Xg + j0, n, Xg, n, n2, s, ozstat, launches);
@@ -520,7 +559,7 @@ extern "C" size_t tups_bse_lu_split_workspace(int n_inst, const int* n, int slic
 extern "C" int tups_bse_lu_split_batched(int n_inst, const int* n, const int* nl, const double* scale,
                                          const double* gamma, const double* chi, double* out, int want_phi,
                                          int slices, double tol, int max_refine, void* work, size_t work_bytes,
-                                         int* refinements, double* correction, int* status, void* stream) {
+                                         int* refinements, double* residual, int* status, void* stream) {
   using namespace tups;
   if (n_inst < 1 || !n || !nl || !scale || !gamma || !chi || !out || !work) return TUPS_ERR_BADARG;
   if (slices < 2 || slices > 8 || max_refine < 0 || !(tol > 0.0)) return TUPS_ERR_BADARG;
@@ -556,7 +595,7 @@ extern "C" int tups_bse_lu_split_batched(int n_inst, const int* n, const int* nl
     p += L.ipiv;
     LsDesc* desc = (LsDesc*)p;
     p += L.desc;
-    unsigned long long* norms = (unsigned long long*)p;  // dmax[b], xmax[b]
+    unsigned long long* norms = (unsigned long long*)p;  // max|R_i| [b], max|Gamma_i| [b]
     p += L.norms;
     int* stat = (int*)p;
     double* ozstat = (double*)(((uintptr_t)(stat + b) + 7) & ~(uintptr_t)7);
@@ -571,11 +610,13 @@ extern "C" int tups_bse_lu_split_batched(int n_inst, const int* n, const int* nl
     }
     const size_t n2 = (size_t)nn * nn;
     const dim3 eg((unsigned)std::min<size_t>((n2 + LS_THREADS - 1) / LS_THREADS, 512), b);
-    k_ls_form<<<eg, LS_THREADS, 0, st>>>(desc, G, CH, Gg, Xg, Ag, nn);
+    if (cudaMemsetAsync(norms, 0, 2 * b * sizeof(unsigned long long), st) != cudaSuccess) return TUPS_ERR_CUDA;
+    k_ls_form<<<eg, LS_THREADS, 0, st>>>(desc, G, CH, Gg, Xg, Ag, norms + b, nn);
     // P A = L U
     for (int j0 = 0; j0 < nn; j0 += LS_NB) {
       const int jb = std::min(LS_NB, nn - j0), je = j0 + jb;
       k_ls_panel<<<b, LS_THREADS, 0, st>>>(Ag, ipiv, stat, nn, j0, jb);
+      if (jb < nn) k_ls_rows<<<dim3((nn + LS_COLS - 1) / LS_COLS, b), LS_COLS, 0, st>>>(Ag, ipiv, nn, j0, jb);
       if (je < nn) {
         int rc = ls_gemm_sub(st, ozw, b, nn - je, nn - je, jb, Ag + je + (size_t)nn * j0, nn, Ag + j0 + (size_t)nn * je,
                              nn, Ag + je + (size_t)nn * je, nn, (long long)n2, slices, ozstat, &launches);
@@ -585,37 +626,36 @@ extern "C" int tups_bse_lu_split_batched(int n_inst, const int* n, const int* nl
     if (cudaGetLastError() != cudaSuccess) return TUPS_ERR_CUDA;
     int rc = ls_solve(st, Ag, Xg, ipiv, ozw, b, nn, slices, ozstat, &launches);
     if (rc) return rc;
+    // refinement: residual in FP64; stop once max|R_i| <= tol max|Gamma_i| for
+    // every instance of the group, else correct with the split-precision factors
     int steps = 0;
-    double worst = 0.0;
-    for (; steps < max_refine; steps++) {
+    const int tiles = ((nn + RS_BM - 1) / RS_BM) * ((nn + RS_BN - 1) / RS_BN);
+    std::vector<unsigned long long> hn(2 * b);
+    std::vector<double> rel(b, 0.0);
+    for (;;) {
+      if (cudaMemsetAsync(norms, 0, b * sizeof(unsigned long long), st) != cudaSuccess) return TUPS_ERR_CUDA;
       k_ls_chimul<<<eg, LS_THREADS, 0, st>>>(desc, CH, Xg, Yg, nn);
-      const int tiles = ((nn + RS_BM - 1) / RS_BM) * ((nn + RS_BN - 1) / RS_BN);
-      k_ls_resid<<<dim3(tiles, b), 128, 0, st>>>(desc, Gg, Yg, Xg, Rg, nn);
-      rc = ls_solve(st, Ag, Rg, ipiv, ozw, b, nn, slices, ozstat, &launches);
-      if (rc) return rc;
-      if (cudaMemsetAsync(norms, 0, 2 * b * sizeof(unsigned long long), st) != cudaSuccess) return TUPS_ERR_CUDA;
-      k_ls_update<<<eg, LS_THREADS, 0, st>>>(Xg, Rg, norms, norms + b, nn);
+      k_ls_resid<<<dim3(tiles, b), 128, 0, st>>>(desc, Gg, Yg, Xg, Rg, norms, nn);
       if (cudaGetLastError() != cudaSuccess) return TUPS_ERR_CUDA;
-      std::vector<unsigned long long> hn(2 * b);
       if (cudaMemcpyAsync(hn.data(), norms, 2 * b * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st) !=
               cudaSuccess ||
           cudaStreamSynchronize(st) != cudaSuccess) {
         cudaGetLastError();
         return TUPS_ERR_CUDA;
       }
-      worst = 0.0;
+      double worst = 0.0;
       for (int k = 0; k < b; k++) {
-        double dm, xm;
-        std::memcpy(&dm, &hn[k], sizeof(double));
-        std::memcpy(&xm, &hn[b + k], sizeof(double));
-        const double r = xm > 0.0 ? dm / xm : dm;
-        if (correction) correction[idx[k]] = r;
-        worst = std::max(worst, r);
+        double rm, gm;
+        std::memcpy(&rm, &hn[k], sizeof(double));
+        std::memcpy(&gm, &hn[b + k], sizeof(double));
+        rel[k] = gm > 0.0 ? rm / gm : rm;
+        worst = std::max(worst, rel[k]);
       }
-      if (worst <= tol) {
-        steps++;
-        break;
-      }
+      if (worst <= tol || steps >= max_refine) break;
+      rc = ls_solve(st, Ag, Rg, ipiv, ozw, b, nn, slices, ozstat, &launches);
+      if (rc) return rc;
+      k_ls_update<<<eg, LS_THREADS, 0, st>>>(Xg, Rg, nn);
+      steps++;
     }
     k_ls_scatter<<<eg, LS_THREADS, 0, st>>>(desc, Xg, Gg, OUT, nn, want_phi);
     std::vector<int> hs(b);
@@ -629,7 +669,7 @@ extern "C" int tups_bse_lu_split_batched(int n_inst, const int* n, const int* nl
     for (int k = 0; k < b; k++) {
       if (status) status[idx[k]] = hs[k];
       if (refinements) refinements[idx[k]] = steps;
-      if (max_refine == 0 && correction) correction[idx[k]] = -1.0;
+      if (residual) residual[idx[k]] = rel[k];
     }
     if (ozflag != 0.0) return TUPS_ERR_TIMEOUT;
   }

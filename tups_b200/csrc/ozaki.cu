@@ -23,6 +23,7 @@
 #include <cuda.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 
 #include "tups_device.cuh"
@@ -244,16 +245,21 @@ __device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
+// SM cycles a wait of the work loop may take before the CTA gives up
+// (about 2 s at 1.965 GHz); the waits of the abort path itself, for copies
+// and MMAs already in flight, always use this default
+constexpr long long OZ_WAIT_CYCLES = 4000000000LL;
+
 // bounded wait: false when the CTA's abort flag is set (honor_abort) or
-// about 2 s pass, in which case the abort flag is set
+// `limit` SM cycles pass, in which case the abort flag is set
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
-                                          bool honor_abort = true) {
+                                          bool honor_abort = true, long long limit = OZ_WAIT_CYCLES) {
   const long long t0 = clock64();
   for (uint32_t it = 0;; it++) {
     if (mbar_try(bar, parity)) return true;
     if ((it & 255) == 255) {
       if (honor_abort && *abort_flag) return false;
-      if (clock64() - t0 > 4000000000LL) {
+      if (clock64() - t0 > limit) {
         *abort_flag = 1;
         return false;
       }
@@ -346,6 +352,8 @@ struct OzGemm {
   double scale[4];
   double omf;
   int q_begin;
+  long long wait_cycles;  // limit of the work loop's waits
+  int stall_test;         // 1: the MMA warp first waits on a barrier nothing signals
 };
 
 __device__ __forceinline__ void tc_ld8(uint32_t taddr, int32_t* v) {
@@ -358,6 +366,7 @@ __global__ void __launch_bounds__(OZ_THREADS2, 1)
     k_oz_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, OzGemm P) {
   extern __shared__ uint8_t oz_dyn[];
   __shared__ uint64_t full_bar[OZ_STAGES], empty_bar[OZ_STAGES], accf_bar[OZ_NBUF], acce_bar[OZ_NBUF], done_bar;
+  __shared__ uint64_t never_bar;  // initialised, never arrived on: the stall test waits here
   __shared__ uint32_t tmem_base_sh;
   __shared__ volatile int abort_sh;
   __shared__ int issued_sh, consumed_sh;
@@ -380,6 +389,7 @@ __global__ void __launch_bounds__(OZ_THREADS2, 1)
       mbar_init(&acce_bar[i], OZ_DRAIN_WARPS * 32);
     }
     mbar_init(&done_bar, 1);
+    mbar_init(&never_bar, 1);
     abort_sh = 0;
     issued_sh = 0;
     consumed_sh = 0;
@@ -410,7 +420,7 @@ __global__ void __launch_bounds__(OZ_THREADS2, 1)
             const int ya = (inst * P.s + i) * P.M + m0;
             const int yb = (inst * P.s + (d - i)) * Np + n0;
             for (int kc = 0; kc < P.kchunks; kc++) {
-              if (!mbar_wait(&empty_bar[stage], phase ^ 1u, &abort_sh)) {
+              if (!mbar_wait(&empty_bar[stage], phase ^ 1u, &abort_sh, true, P.wait_cycles)) {
                 ok = false;
                 break;
               }
@@ -437,11 +447,14 @@ __global__ void __launch_bounds__(OZ_THREADS2, 1)
       int consumed = 0;
       int nacc = 0;  // accumulations issued so far (one per tile and diagonal)
       bool ok = true;
+      // failure-path test: a wait that can only run out, before any MMA
+      if (P.stall_test) ok = mbar_wait(&never_bar, 0, &abort_sh, true, P.wait_cycles);
       for (int t = blockIdx.x; t < P.tiles && ok; t += gridDim.x)
         for (int d = 0; d < P.s && ok; d++, nacc++) {
           const int buf = nacc % OZ_NBUF;
           if (nacc >= OZ_NBUF &&
-              !mbar_wait(&acce_bar[buf], (uint32_t)((nacc - OZ_NBUF) / OZ_NBUF) & 1u, &abort_sh)) {
+              !mbar_wait(&acce_bar[buf], (uint32_t)((nacc - OZ_NBUF) / OZ_NBUF) & 1u, &abort_sh, true,
+                         P.wait_cycles)) {
             ok = false;
             break;
           }
@@ -450,7 +463,7 @@ __global__ void __launch_bounds__(OZ_THREADS2, 1)
           uint32_t accum = 0;
           for (int i = 0; i <= d && ok; i++)
             for (int kc = 0; kc < P.kchunks; kc++) {
-              if (!mbar_wait(&full_bar[stage], phase, &abort_sh)) {
+              if (!mbar_wait(&full_bar[stage], phase, &abort_sh, true, P.wait_cycles)) {
                 ok = false;
                 break;
               }
@@ -492,7 +505,7 @@ __global__ void __launch_bounds__(OZ_THREADS2, 1)
       for (int c = 0; c < OZ_HALF; c++) acc[c] = 0.0;
       for (int d = 0; d < P.s; d++, nacc++) {
         const int buf = nacc % OZ_NBUF;
-        if (!mbar_wait(&accf_bar[buf], (uint32_t)(nacc / OZ_NBUF) & 1u, &abort_sh)) {
+        if (!mbar_wait(&accf_bar[buf], (uint32_t)(nacc / OZ_NBUF) & 1u, &abort_sh, true, P.wait_cycles)) {
           ok = false;
           break;
         }
@@ -580,6 +593,11 @@ __global__ void __launch_bounds__(OZ_THREADS2, 1)
 }
 
 // ---- host side ----------------------------------------------------------------------
+// the work loop's wait limit (0: OZ_WAIT_CYCLES) and a pending stall test,
+// set by tups_set_split_wait; the stall test applies to the next launch only
+static std::atomic<long long> g_oz_wait_cycles{0};
+static std::atomic<int> g_oz_stall_test{0};
+
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -705,6 +723,11 @@ int oz_run(OzRun& R, cudaStream_t stream, long long* launches) {
   }
   P.omf = R.omf;
   P.q_begin = R.q_begin;
+  {
+    const long long lim = g_oz_wait_cycles.load();
+    P.wait_cycles = lim > 0 ? lim : OZ_WAIT_CYCLES;
+    P.stall_test = g_oz_stall_test.exchange(0);
+  }
   CUtensorMap ta, tb;
   if (!make_map(&ta, R.a_slices, (long long)batch * s * M, Kpad, OZ_BM)) return TUPS_ERR_CUDA;
   if (!make_map(&tb, R.b_slices, (long long)batch * s * 2 * N, Kpad, P.n_tile)) return TUPS_ERR_CUDA;
@@ -766,4 +789,17 @@ extern "C" int tups_zgemm_split(int batch, int M, int N, int K, const double* A,
   if (cudaMemcpyAsync(&flag, status, sizeof(double), cudaMemcpyDeviceToHost, st) != cudaSuccess) return TUPS_ERR_CUDA;
   if (cudaStreamSynchronize(st) != cudaSuccess) return TUPS_ERR_CUDA;
   return flag != 0.0 ? TUPS_ERR_TIMEOUT : TUPS_OK;
+}
+
+// Failure detection of the split GEMM's bounded device waits.  cycles > 0
+// sets how many SM cycles a wait of the work loop may take (0 restores the
+// default, about 2 s); stall_test = 1 makes the next split GEMM launch wait
+// first on a barrier that nothing signals, so its bounded wait runs out: the
+// kernel then drains its copies in flight, frees its tensor memory, returns,
+// and the call reports TUPS_ERR_TIMEOUT; the launch after it runs normally.
+extern "C" int tups_set_split_wait(long long cycles, int stall_test) {
+  if (cycles < 0) return TUPS_ERR_BADARG;
+  tups::g_oz_wait_cycles.store(cycles);
+  tups::g_oz_stall_test.store(stall_test ? 1 : 0);
+  return TUPS_OK;
 }
