@@ -439,12 +439,11 @@ static int build_pae_lists(tups_ctx* ctx) {
 // in how the (target, element) rows and the (momentum, (l1, l2)) columns are
 // spread over CTAs and warps; every output element is still summed over K in
 // the same order, so all candidates write the same bits.  Index 0 is the
-// default when the tuner is off.  Measured on a B200 before the tuner: at
-// Nl^2 = 25 three momenta side by side (75 of 80 columns used) 1.76 ms at
-// 8x8 / Nl = 5 against 1.89 ms with one momentum per CTA; at Nl^2 = 81 one
-// momentum per 96-column CTA, two CTAs per SM, 482 ms at 16x16 / Nl = 9
-// (one 16-warp CTA of 64 elements per SM 540 ms, 64 elements x 48 columns in
-// two chunks 491 ms).
+// default when the tuner is off: the tuner's pick on a B200, flat 64-column
+// tiles, at 8x8 / Nl = 5 (1.677 ms against 1.760 ms for three momenta side
+// by side in 80 columns, 1.754 flat 80, 1.734 flat 48) and at 16x16 / Nl = 9
+// (403 ms against 481 ms for one momentum per 96-column CTA, 406 flat 80,
+// 411 flat 96, 428 flat 112; two CTAs per SM throughout).
 struct PaeCand {
   const char* name;
   int (*run)(tups_ctx*, const PaePtrs&, int, int, int);
@@ -456,16 +455,16 @@ static const PaeCand kPaeNl1[] = {
     {"q1_bn8_tn1", run_pae<1, 1, 4, 2, 1>, 8},
 };
 static const PaeCand kPaeNl5[] = {
+    {"flat_bn64_tn4", run_pae<4, 2, 4, 2, 0>, 64},
     {"q3_bn80_tn5", run_pae<5, 2, 4, 2, 3>, 80},
     {"flat_bn80_tn5", run_pae<5, 2, 4, 2, 0>, 80},
-    {"flat_bn64_tn4", run_pae<4, 2, 4, 2, 0>, 64},
     {"flat_bn48_tn3", run_pae<3, 2, 4, 2, 0>, 48},
 };
 static const PaeCand kPaeWide[] = {
-    {"flat_bn96_tn6", run_pae<6, 2, 4, 2, 0>, 96},
+    {"flat_bn64_tn4", run_pae<4, 2, 4, 2, 0>, 64},
     {"q1_bn96_tn6", run_pae<6, 2, 4, 2, 1>, 96},
     {"flat_bn80_tn5", run_pae<5, 2, 4, 2, 0>, 80},
-    {"flat_bn64_tn4", run_pae<4, 2, 4, 2, 0>, 64},
+    {"flat_bn96_tn6", run_pae<6, 2, 4, 2, 0>, 96},
     {"flat_bn112_tn7", run_pae<7, 2, 4, 2, 0>, 112},
 };
 
