@@ -184,15 +184,22 @@ def oracle_params(wl: dict):
     return O.Params(**kw)
 
 
+CPU_PORT_SAMPLE = ("oracle port on the host cores: the numpy restatement of the reference with its crossing "
+                   "and Phi(R) compiled (C++/OpenMP loop nests, oracle/port) and the BSE's ZGEMMs on OpenBLAS")
+
+
 def cpu_oracle_seconds_per_iteration(wl: dict, timed_iterations: int = 1, warm_iterations: int = 1):
-    """Time the oracle port: warm (untimed) iterations, then timed ones."""
+    """Time the oracle port (oracle.port.iteration): warm (untimed)
+    iterations, then timed ones."""
     from oracle import tups_oracle as O
+    from oracle import port as OP
+    OP.threads(os.cpu_count() or 1)
     st = O.initialize(oracle_params(wl))
     for ite in range(warm_iterations):
-        O.iteration(st, ite)
+        OP.iteration(st, ite)
     t0 = time.perf_counter()
     for ite in range(warm_iterations, warm_iterations + timed_iterations):
-        O.iteration(st, ite)
+        OP.iteration(st, ite)
     return (time.perf_counter() - t0) / timed_iterations
 
 
@@ -234,7 +241,7 @@ def run_reference(args, wl_name: str, wl: dict):
         return
     steps, warm = args.steps, args.warmup
     spi = cpu_oracle_seconds_per_iteration(wl, timed_iterations=steps, warm_iterations=warm)
-    cores = blas_threads()
+    cores = max(blas_threads(), os.cpu_count() or 1)
     tools = fortran_toolchain()
     line = {
         "impl": "reference", "metric": METRIC, "metric_full": METRIC_FULL, "value": spi, "unit": "s/iter",
@@ -242,8 +249,7 @@ def run_reference(args, wl_name: str, wl: dict):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": workload_config(wl_name, wl, ws),
         "cpu_baseline": {"value": spi, "unit": "s/iter", "cores": cores, "kind": "port",
-                         "sample": f"{steps} oracle iteration(s) after {warm} untimed; numpy/OpenBLAS "
-                                   "restatement of the reference"},
+                         "sample": f"{steps} iteration(s) after {warm} untimed; " + CPU_PORT_SAMPLE},
         "reference_toolchain": tools,
         "reference_note": ("the Fortran reference needs mpif90 + MKL + HDF5-Fortran; none of the compilers "
                            "probed here is present" if not any(tools.values()) else
@@ -374,10 +380,9 @@ def run_tups(args, wl_name: str, wl: dict):
         target = target_record(device)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        sec = cpu_oracle_seconds_per_iteration(wl)
-        cpu = {"value": sec, "unit": "s/iter", "cores": blas_threads(), "kind": "port",
-               "sample": "1 oracle iteration (ite 1, after an untimed ite 0) of the same workload; "
-                         "numpy/OpenBLAS restatement of the reference"}
+        sec = cpu_oracle_seconds_per_iteration(wl, timed_iterations=2)
+        cpu = {"value": sec, "unit": "s/iter", "cores": max(blas_threads(), os.cpu_count() or 1), "kind": "port",
+               "sample": "2 iterations (ite 1-2, after an untimed ite 0) of the same workload; " + CPU_PORT_SAMPLE}
     if rank == 0:
         line = {
             "metric": METRIC, "metric_full": METRIC_FULL, "value": value, "unit": "s/iter", "n_gpus": ws,

@@ -159,7 +159,9 @@ __global__ void k_pae_base(PaePtrs P, const int* __restrict__ ibz, int Nz, int N
 // are applied when the MMA fragments are read, so no warp waits on a gather
 // between K steps.  The per-k offsets into Phi(R) and the signs s(l3) s(l4)
 // are tabulated once per CTA.
-template <int TN, int WN, int RW, int STG, int QN>
+// G3: three real DMMA products per complex one (P1 = Xr Mr, P2 = Xi Mi,
+// P3 = (Xr + Xi)(Mr + Mi); Re = P1 - P2, Im = P3 - P1 - P2), else four.
+template <int TN, int WN, int RW, int STG, int QN, bool G3 = false>
 __global__ void __launch_bounds__(32 * RW * WN, RW * WN == 8 ? (TN <= 2 ? PAE_MIN_BLOCKS : 2) : 1)
     k_pae_mma(PaePtrs P, const int4* __restrict__ elems, const int* __restrict__ counts,
               const int* __restrict__ ibz, const int* __restrict__ signs, int Nz, int Nf, int Nl, int NIBZ, int NR,
@@ -287,11 +289,15 @@ __global__ void __launch_bounds__(32 * RW * WN, RW * WN == 8 ? (TN <= 2 ? PAE_MI
   const int er = (wr * 16) % E + gid;       // its elements er and er + 8
   const double fa = fac[0][tgt], fb = fac[1][tgt];
   const bool tr0 = e_tr[er] != 0, tr1 = e_tr[er + 8] != 0;
-  double cre[TN][4], cim[TN][4];
+  // four products: cre, cim; three: P1 in cre, P2 in cim, P3 in c3
+  double cre[TN][4], cim[TN][4], c3[G3 ? TN : 1][4];
 #pragma unroll
   for (int j = 0; j < TN; j++)
 #pragma unroll
-    for (int x = 0; x < 4; x++) cre[j][x] = cim[j][x] = 0.0;
+    for (int x = 0; x < 4; x++) {
+      cre[j][x] = cim[j][x] = 0.0;
+      if (G3) c3[G3 ? j : 0][x] = 0.0;
+    }
 
   // fragment value of element e at k: fa x0 + fb x1, conjugated with sign
   // s(l3) s(l4) for time-reversed elements
@@ -330,20 +336,37 @@ __global__ void __launch_bounds__(32 * RW * WN, RW * WN == 8 ? (TN <= 2 ? PAE_MI
       xval(cX, k8 + tig + 4, er, tr0, sb, are[2], aim[2]);
       xval(cX, k8 + tig + 4, er + 8, tr1, sb, are[3], aim[3]);
 #pragma unroll
-      for (int x = 0; x < 4; x++) anim[x] = -aim[x];
+      for (int x = 0; x < 4; x++) anim[x] = G3 ? are[x] + aim[x] : -aim[x];  // G3: the sum Xr + Xi
 #pragma unroll
       for (int j = 0; j < TN; j++) {
         const int nb = (wc * TN + j) * 8 + gid;
         const cplx w0 = cB[nb * PAE_LDB + k8 + tig], w1 = cB[nb * PAE_LDB + k8 + tig + 4];
         const double bre[2] = {w0.x, w1.x}, bim[2] = {w0.y, w1.y};
-        dmma_16x8x8(cre[j], are, bre);
-        dmma_16x8x8(cre[j], anim, bim);
-        dmma_16x8x8(cim[j], are, bim);
-        dmma_16x8x8(cim[j], aim, bre);
+        if (G3) {
+          const double bsum[2] = {w0.x + w0.y, w1.x + w1.y};
+          dmma_16x8x8(cre[j], are, bre);
+          dmma_16x8x8(cim[j], aim, bim);
+          dmma_16x8x8(c3[G3 ? j : 0], anim, bsum);
+        } else {
+          dmma_16x8x8(cre[j], are, bre);
+          dmma_16x8x8(cre[j], anim, bim);
+          dmma_16x8x8(cim[j], are, bim);
+          dmma_16x8x8(cim[j], aim, bre);
+        }
       }
     }
   }
   asm volatile("cp.async.wait_group 0;\n" ::);
+  if (G3) {
+#pragma unroll
+    for (int j = 0; j < TN; j++)
+#pragma unroll
+      for (int x = 0; x < 4; x++) {
+        const double p1 = cre[j][x], p2 = cim[j][x];
+        cre[j][x] = p1 - p2;
+        cim[j][x] = c3[G3 ? j : 0][x] - p1 - p2;
+      }
+  }
 
   // epilogue: F_target += C / Nx on the listed elements (each element is in
   // a family's list once, so a pass writes it at most once)
@@ -367,7 +390,7 @@ __global__ void __launch_bounds__(32 * RW * WN, RW * WN == 8 ? (TN <= 2 ? PAE_MI
     }
 }
 
-template <int TN, int WN, int RW, int STG, int QN = 1>
+template <int TN, int WN, int RW, int STG, int QN = 1, bool G3 = false>
 static int run_pae(tups_ctx* ctx, const PaePtrs& P, int nchunks, int fam, int max_count) {
   const auto& d = ctx->d;
   constexpr int BN = 8 * TN * WN;
@@ -377,7 +400,7 @@ static int run_pae(tups_ctx* ctx, const PaePtrs& P, int nchunks, int fam, int ma
   const int Kpad = (K + PAE_BK - 1) / PAE_BK * PAE_BK;
   const size_t sm = (size_t)(STG * 2 * PAE_BK * LDX + STG * BN * PAE_LDB) * sizeof(cplx) +
                     (size_t)Kpad * (sizeof(long long) + sizeof(double));
-  auto kern = k_pae_mma<TN, WN, RW, STG, QN>;
+  auto kern = k_pae_mma<TN, WN, RW, STG, QN, G3>;
   if (sm > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return cuda_check(ctx, e, "k_pae_mma smem attribute");

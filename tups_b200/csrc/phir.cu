@@ -14,53 +14,95 @@ struct PhirPtrs {
   cplx* PhiR[4];
 };
 
-// PhiR_r[(i,j), w, R] = (1/Nx) sum_sym sum_Q fac_sym(l_i) fac_sym(l_j)
+// PhiR_r[(i,j), w, R] = (1/Nx) sum_Q sum_{sym in star(Q)} fac_sym(l_i) fac_sym(l_j)
 //     Phi_r[(lsym(l_i), nu_i), (lsym(l_j), nu_j), (Q, w)] expSqR(Q, R, sym)
-// One thread per (i, j) entry, all R at once; symmetries outside the star of
-// Q carry expSqR = 0 and are skipped.
-__global__ void k_phir(PhirPtrs P, const cplx* __restrict__ expSqR, const int* __restrict__ symlist,
-                       const int* __restrict__ lsym, const double* __restrict__ lfac, int Nz, int Nf, int Nl,
-                       int NIBZ, int NR, int slot0, int Nb, double inv_nx) {
-  // the phase tables (expSqR, star lists, l-space maps) of all threads in
-  // shared memory: the inner loop reads only Phi from global memory
+// One thread per (i, j) entry, all R at once.  The (sym, Q) pairs with
+// sym in the star of Q (expSqR = 0 elsewhere; Nc pairs in all) are listed
+// once per CTA with Q outermost, so at any moment the CTAs in flight read
+// the few Nz^2 slices of one or two momenta: every symmetric image of an
+// entry is then an L2 hit and Phi(Q) streams from DRAM once (the slab of all
+// momenta of one (w, r), 239 MB at 16x16 / Nl = 9 / Nf = 64, exceeds L2).
+// Loads are issued four pairs ahead of their FMAs.
+__global__ void __launch_bounds__(256) k_phir(PhirPtrs P, const cplx* __restrict__ expSqR,
+                                              const int* __restrict__ symlist, const int* __restrict__ lsym,
+                                              const double* __restrict__ lfac, int Nz, int Nf, int Nl, int NIBZ,
+                                              int NR, int slot0, int Nb, double inv_nx) {
+  // the phase tables (expSqR, pair list, l-space maps) in shared memory: the
+  // inner loop reads only Phi from global memory
   extern __shared__ __align__(16) unsigned char phir_sm[];
-  cplx* sE = reinterpret_cast<cplx*>(phir_sm);                   // (NIBZ, NR, NS)
-  int* sSym = reinterpret_cast<int*>(sE + (size_t)NIBZ * NR * NS);  // (NS, NIBZ)
+  cplx* sE = reinterpret_cast<cplx*>(phir_sm);                    // (NIBZ, NR, NS)
+  int* sPair = reinterpret_cast<int*>(sE + (size_t)NIBZ * NR * NS);  // sym + NS Q, Q ascending
   __shared__ int sL[NS * 16];
   __shared__ double sF[NS * 16];
+  __shared__ int sNp;
   for (int t = threadIdx.x; t < NIBZ * NR * NS; t += blockDim.x) sE[t] = expSqR[t];
-  for (int t = threadIdx.x; t < NIBZ * NS; t += blockDim.x) sSym[t] = symlist[t];
   for (int t = threadIdx.x; t < NS * Nl; t += blockDim.x) {
     sL[t] = lsym[t];
     sF[t] = lfac[t];
   }
+  const int w = blockIdx.y;  // 0..Nf/2-1
+  const int nh = Nf / 2;
+  if (threadIdx.x == 0) {
+    int np = 0;
+    for (int Q = 0; Q < NIBZ; Q++) {
+      // slot (Q, w) is global slot Q nh + w; a sharded context sums its own
+      const int lq = Q * nh + w - slot0;
+      if (lq < 0 || lq >= Nb) continue;
+      for (int sy = 0; sy < NS; sy++)
+        if (symlist[NS * Q + sy]) sPair[np++] = sy + NS * Q;
+    }
+    sNp = np;
+  }
   __syncthreads();
   const int r = blockIdx.z;
-  const int w = blockIdx.y;  // 0..Nf/2-1
   const size_t n2 = (size_t)Nz * Nz;
   const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= n2) return;
   const int i = (int)(e % Nz), j = (int)(e / Nz);
   const int li = i / Nf, ni = i % Nf, lj = j / Nf, nj = j % Nf;
-  const int nh = Nf / 2;
+  // per symmetry: offset of the permuted entry and its sign
+  long long off[NS];
+  double fac[NS];
+#pragma unroll
+  for (int sy = 0; sy < NS; sy++) {
+    off[sy] = (long long)(sL[sy + NS * li] * Nf + ni) + (long long)Nz * (sL[sy + NS * lj] * Nf + nj);
+    fac[sy] = sF[sy + NS * li] * sF[sy + NS * lj];
+  }
   cplx acc[8];
 #pragma unroll
   for (int R = 0; R < 8; R++) acc[R] = cmk(0.0, 0.0);
   const cplx* G = P.G[r];
-  for (int s = 0; s < NS; s++) {
-    const int lis = sL[s + NS * li], ljs = sL[s + NS * lj];
-    const double f = sF[s + NS * li] * sF[s + NS * lj];
-    const cplx* src = G + (size_t)(lis * Nf + ni) + (size_t)Nz * (ljs * Nf + nj);
-    for (int Q = 0; Q < NIBZ; Q++) {
-      if (!sSym[NS * Q + s]) continue;
-      // slot (Q, w) is global slot Q nh + w; a sharded context sums its own
-      const int lq = Q * nh + w - slot0;
-      if (lq < 0 || lq >= Nb) continue;
-      const cplx v = cscale(__ldg(src + n2 * (size_t)lq), f);
-      const cplx* eq = sE + Q + (size_t)NIBZ * NR * s;
+  const int np = sNp;
+  constexpr int U = 4;
+  for (int p0 = 0; p0 < np; p0 += U) {
+    cplx v[U];
+    int pr[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      pr[u] = p0 + u < np ? sPair[p0 + u] : -1;
+      v[u] = cmk(0.0, 0.0);
+      if (pr[u] >= 0) {
+        const int sy = pr[u] % NS, Q = pr[u] / NS;
+        long long o = off[0];
+#pragma unroll
+        for (int t = 1; t < NS; t++)
+          if (t == sy) o = off[t];
+        v[u] = __ldg(G + o + (long long)n2 * (Q * nh + w - slot0));
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      if (pr[u] < 0) continue;
+      const int sy = pr[u] % NS, Q = pr[u] / NS;
+      double f = fac[0];
+#pragma unroll
+      for (int t = 1; t < NS; t++)
+        if (t == sy) f = fac[t];
+      const cplx vv = cscale(v[u], f);
+      const cplx* eq = sE + Q + (size_t)NIBZ * NR * sy;
 #pragma unroll
       for (int R = 0; R < 8; R++)
-        if (R < NR) acc[R] = cfma(v, eq[(size_t)NIBZ * R], acc[R]);
+        if (R < NR) acc[R] = cfma(vv, eq[(size_t)NIBZ * R], acc[R]);
     }
   }
   cplx* out = P.PhiR[r];
