@@ -749,27 +749,32 @@ def run_zgemm_split(args):
     zgemm_ms = time_cublas()
     flops = 8.0 * M * N * K * batch
     out = {}
-    for s in args.slices:
-        wsz = lib.tups_zgemm_split_workspace(batch, M, N, K, s)
-        work = torch.empty(wsz, dtype=torch.uint8, device="cuda")
-        cargs = (batch, M, N, K, C.c_void_p(A.data_ptr()), C.c_void_p(B.data_ptr()), C.c_void_p(Cm.data_ptr()), s,
-                 C.c_void_p(work.data_ptr()), wsz, C.c_void_p(stream.cuda_stream))
-        rc = lib.tups_zgemm_split(*cargs)
-        if rc:
-            raise RuntimeError(f"tups_zgemm_split failed with {rc}")
-        err = float((Cm[0].transpose(0, 1) - ref).abs().max() / ref.abs().max())
-        torch.cuda.synchronize()
-        e0.record()
-        for _ in range(reps):
-            lib.tups_zgemm_split(*cargs)
-        e1.record()
-        torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1) / reps
-        pairs = s * (s + 1) // 2
-        out[str(s)] = {"ms": ms, "effective_tflops": flops / ms / 1e9,
-                       "int8_tops": 2.0 * pairs * M * (2 * N) * (2 * K) * batch / ms / 1e9,
-                       "rel_err_vs_fp64": err}
-        del work
+    for nt in args.n_tile:
+        if lib.tups_set_split_tile(nt):
+            raise RuntimeError(f"tups_set_split_tile({nt}) refused")
+        for s in args.slices:
+            wsz = lib.tups_zgemm_split_workspace(batch, M, N, K, s)
+            work = torch.empty(wsz, dtype=torch.uint8, device="cuda")
+            cargs = (batch, M, N, K, C.c_void_p(A.data_ptr()), C.c_void_p(B.data_ptr()), C.c_void_p(Cm.data_ptr()),
+                     s, C.c_void_p(work.data_ptr()), wsz, C.c_void_p(stream.cuda_stream))
+            rc = lib.tups_zgemm_split(*cargs)
+            if rc:
+                raise RuntimeError(f"tups_zgemm_split failed with {rc}")
+            err = float((Cm[0].transpose(0, 1) - ref).abs().max() / ref.abs().max())
+            torch.cuda.synchronize()
+            e0.record()
+            for _ in range(reps):
+                lib.tups_zgemm_split(*cargs)
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / reps
+            pairs = s * (s + 1) // 2
+            key = str(s) if len(args.n_tile) == 1 else f"{s}/n_tile={nt or 'auto'}"
+            out[key] = {"ms": ms, "effective_tflops": flops / ms / 1e9,
+                        "int8_tops": 2.0 * pairs * M * (2 * N) * (2 * K) * batch / ms / 1e9,
+                        "rel_err_vs_fp64": err}
+            del work
+    lib.tups_set_split_tile(0)
     zgemm_ms = min(zgemm_ms, time_cublas())
     line = {"metric": "split ZGEMM effective TFLOP/s", "unit": "TFLOP/s", "workload": ZGEMM_WORKLOAD,
             "config": {"Nz": Nz, "batch": batch, "M": M, "N": N, "K": K}, "steps": reps,
@@ -787,6 +792,8 @@ def main():
     ap.add_argument("--nz", type=int, default=576, help="zgemm_split: M = N = Nz, K = 2 Nz")
     ap.add_argument("--batch", type=int, default=64, help="zgemm_split: batch entries")
     ap.add_argument("--slices", type=int, nargs="+", default=[2, 3, 4, 5, 6, 7, 8], help="zgemm_split: slice counts")
+    ap.add_argument("--n-tile", type=int, nargs="+", default=[0],
+                    help="zgemm_split: column tiles of the split GEMM to compare (0 = automatic)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-split", action="store_true", help="skip the split-precision iterations")
     ap.add_argument("--no-graph", action="store_true", help="launch the timed iterations kernel by kernel")

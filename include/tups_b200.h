@@ -262,6 +262,12 @@ int tups_zgemm_split(int batch, int M, int N, int K, const double* A, const doub
  * timeout path that faults nothing); later launches run normally.
  * Process-wide. */
 int tups_set_split_wait(long long cycles, int stall_test);
+/* Column tile of the split GEMM (real columns of [Re B | Im B] per CTA tile):
+ * n_tile = 16, 32, ..., 128 fixes it, 0 restores the automatic choice (the
+ * fewest tiles, then the widest).  Every tile shape gives the same bits (the
+ * integer slice sums are exact and the FP64 folding order is fixed).
+ * Process-wide; no counterpart in the reference. */
+int tups_set_split_tile(int n_tile);
 
 /* ---- tile-shape tuner -------------------------------------------------------
  * No counterpart in the reference.  The first FP64 BSE GEMM and the first

@@ -597,6 +597,7 @@ __global__ void __launch_bounds__(OZ_THREADS2, 1)
 // set by tups_set_split_wait; the stall test applies to the next launch only
 static std::atomic<long long> g_oz_wait_cycles{0};
 static std::atomic<int> g_oz_stall_test{0};
+static std::atomic<int> g_oz_n_tile{0};  // 0: oz_n_tile
 
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
@@ -703,7 +704,10 @@ int oz_run(OzRun& R, cudaStream_t stream, long long* launches) {
   P.N = N;
   P.s = s;
   P.kchunks = Kpad / OZ_BK;
-  P.n_tile = oz_n_tile(N);
+  {
+    const int nt = g_oz_n_tile.load();
+    P.n_tile = nt > 0 ? nt : oz_n_tile(N);
+  }
   P.m_tiles = (M + OZ_BM - 1) / OZ_BM;
   P.n_tiles = (2 * N + P.n_tile - 1) / P.n_tile;
   if ((long long)batch * P.m_tiles * P.n_tiles >= (1LL << 31)) return TUPS_ERR_BADDIM;
@@ -801,5 +805,11 @@ extern "C" int tups_set_split_wait(long long cycles, int stall_test) {
   if (cycles < 0) return TUPS_ERR_BADARG;
   tups::g_oz_wait_cycles.store(cycles);
   tups::g_oz_stall_test.store(stall_test ? 1 : 0);
+  return TUPS_OK;
+}
+
+extern "C" int tups_set_split_tile(int n_tile) {
+  if (n_tile < 0 || n_tile > tups::OZ_MAX_NT || n_tile % 16) return TUPS_ERR_BADARG;
+  tups::g_oz_n_tile.store(n_tile);
   return TUPS_OK;
 }

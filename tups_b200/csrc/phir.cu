@@ -3,6 +3,7 @@
 //   calculate_expSqR / calculate_expqSR (SRC/parquet_PhiR.f90:360-435)
 //   calc_M_* (SRC/parquet_EQMatrix.f90:21-360), evaluated per IBZ momentum
 #include <cmath>
+#include <string>
 #include <vector>
 
 #include "tups_device.cuh"
@@ -16,97 +17,191 @@ struct PhirPtrs {
 
 // PhiR_r[(i,j), w, R] = (1/Nx) sum_Q sum_{sym in star(Q)} fac_sym(l_i) fac_sym(l_j)
 //     Phi_r[(lsym(l_i), nu_i), (lsym(l_j), nu_j), (Q, w)] expSqR(Q, R, sym)
-// One thread per (i, j) entry, all R at once.  The (sym, Q) pairs with
-// sym in the star of Q (expSqR = 0 elsewhere; Nc pairs in all) are listed
-// once per CTA with Q outermost, so at any moment the CTAs in flight read
-// the few Nz^2 slices of one or two momenta: every symmetric image of an
-// entry is then an L2 hit and Phi(Q) streams from DRAM once (the slab of all
-// momenta of one (w, r), 239 MB at 16x16 / Nl = 9 / Nf = 64, exceeds L2).
-// Loads are issued four pairs ahead of their FMAs.
-__global__ void __launch_bounds__(256) k_phir(PhirPtrs P, const cplx* __restrict__ expSqR,
-                                              const int* __restrict__ symlist, const int* __restrict__ lsym,
-                                              const double* __restrict__ lfac, int Nz, int Nf, int Nl, int NIBZ,
-                                              int NR, int slot0, int Nb, double inv_nx) {
-  // the phase tables (expSqR, pair list, l-space maps) in shared memory: the
-  // inner loop reads only Phi from global memory
-  extern __shared__ __align__(16) unsigned char phir_sm[];
-  cplx* sE = reinterpret_cast<cplx*>(phir_sm);                    // (NIBZ, NR, NS)
-  int* sPair = reinterpret_cast<int*>(sE + (size_t)NIBZ * NR * NS);  // sym + NS Q, Q ascending
-  __shared__ int sL[NS * 16];
-  __shared__ double sF[NS * 16];
-  __shared__ int sNp;
-  for (int t = threadIdx.x; t < NIBZ * NR * NS; t += blockDim.x) sE[t] = expSqR[t];
-  for (int t = threadIdx.x; t < NS * Nl; t += blockDim.x) {
-    sL[t] = lsym[t];
-    sF[t] = lfac[t];
+// (the reference's symop_arr + FTPhis ZGEMM, parquet_PhiR.f90:196-356; the
+// symmetries outside the star of Q carry expSqR = 0 and are skipped).
+//
+// The symmetry operations permute the form-factor index only, never nu, so
+// every output of the pair (nu_i, nu_j) reads the same Nl x Nl inputs
+// Phi[(a, nu_i), (b, nu_j), Q].  A CTA owns one nu_j, a tile of PH_TI
+// consecutive nu_i and one (w, r).  For each momentum Q of the context it
+// stages Phi[(a, nu_i), (b, nu_j), (Q, w)] for all a, b and the tile's nu_i
+// (Nl^2 runs of PH_TI contiguous complex) in shared memory, double buffered
+// with cp.async, and every symmetric image of Q reads its permuted entries
+// (lsym(l_i), lsym(l_j)) from there: each Phi(Q) element leaves HBM once and
+// the inner loop is FP64 FMAs on shared-memory operands.  Per output the sum
+// runs over Q ascending and, within Q, over the star's symmetries ascending.
+//
+// Thread (pair p = l_i + Nl l_j, lane c < SUB = PH_TI / OPT) owns the OPT
+// outputs nu_i = nu_i0 + c + SUB k, all NR lattice vectors; the phases
+// expSqR(Q, R, sym) of the star pairs sit in shared memory, packed by pair.
+constexpr int PH_TI = 16;
+
+__device__ __forceinline__ void ph_cp_async16(void* sdst, const void* gsrc, bool valid) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(sdst));
+  const unsigned sz = valid ? 16u : 0u;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gsrc), "r"(sz));
+}
+
+// flips the sign of x when bit is set (an integer operation: the FP64 pipe
+// stays with the FMAs)
+__device__ __forceinline__ double ph_sign(double x, unsigned bit) {
+  return __longlong_as_double(__double_as_longlong(x) ^ ((long long)bit << 63));
+}
+
+// threads per CTA the register budget allows (acc is 4 OPT NR registers)
+__host__ __device__ constexpr int phir_max_threads(int opt, int nr) {
+  return nr == 1 ? 1024 : opt == 4 ? 384 : opt == 2 ? 672 : 768;
+}
+
+// stage Phi[(a, ni0 + t), (b, nj)] (t < PH_TI, all a, b < Nl) of one slot
+// into dst[(a + Nl b) PH_TI + t]; src points at element (0, nj) of the
+// slot; entries with ni >= Nf are zero-filled
+__device__ __forceinline__ void ph_stage(cplx* dst, const cplx* src, int n, int Nl, int Nf, int Nz, int ni0) {
+  for (int x = threadIdx.x; x < n; x += blockDim.x) {
+    const int t = x % PH_TI, ab = x / PH_TI;
+    const int a = ab % Nl, b = ab / Nl, ni = ni0 + t;
+    const bool ok = ni < Nf;
+    ph_cp_async16(dst + x, ok ? src + (a * Nf + ni) + (size_t)Nz * Nf * b : src, ok);
   }
-  const int w = blockIdx.y;  // 0..Nf/2-1
+}
+
+template <int OPT, int NR>
+__global__ void __launch_bounds__(phir_max_threads(OPT, NR)) k_phir(PhirPtrs P, const cplx* __restrict__ expSqR,
+                                               const int* __restrict__ symlist, const int* __restrict__ lsym,
+                                               const double* __restrict__ lfac, int Nz, int Nf, int Nl, int NIBZ,
+                                               int npairs, int slot0, int Nb, double inv_nx) {
+  constexpr int SUB = PH_TI / OPT;
+  extern __shared__ __align__(16) unsigned char phir_sm[];
+  const int nl2 = Nl * Nl;
+  cplx* sPhi = reinterpret_cast<cplx*>(phir_sm);          // [2][nl2][PH_TI]
+  cplx* sE = sPhi + (size_t)2 * nl2 * PH_TI;               // [npairs][NR]
+  int* sSym = reinterpret_cast<int*>(sE + (size_t)npairs * NR);  // [npairs] symmetry of pair p
+  int* sBeg = sSym + npairs;                               // [NIBZ + 1] first pair of Q
+  int* sQ = sBeg + NIBZ + 1;                               // [NIBZ] momenta of this context at w
+  __shared__ int sNq;
+
+  const int ntile = (Nf + PH_TI - 1) / PH_TI;
+  const int nj = blockIdx.x / ntile, ni0 = (blockIdx.x % ntile) * PH_TI;
+  const int w = blockIdx.y, r = blockIdx.z;
   const int nh = Nf / 2;
-  if (threadIdx.x == 0) {
-    int np = 0;
-    for (int Q = 0; Q < NIBZ; Q++) {
-      // slot (Q, w) is global slot Q nh + w; a sharded context sums its own
-      const int lq = Q * nh + w - slot0;
-      if (lq < 0 || lq >= Nb) continue;
-      for (int sy = 0; sy < NS; sy++)
-        if (symlist[NS * Q + sy]) sPair[np++] = sy + NS * Q;
+  const int lane = threadIdx.x & 31;
+
+  // star pairs with Q ascending (prefix sums of the star sizes) and the
+  // momenta whose slot (Q, w) this context holds; first warp
+  if (threadIdx.x < 32) {
+    int base = 0, nq = 0;
+    for (int Q0 = 0; Q0 < NIBZ; Q0 += 32) {
+      const int Q = Q0 + lane;
+      unsigned m = 0;
+      bool mine = false;
+      if (Q < NIBZ) {
+#pragma unroll
+        for (int sy = 0; sy < NS; sy++)
+          if (symlist[NS * Q + sy]) m |= 1u << sy;
+        const int lq = Q * nh + w - slot0;
+        mine = lq >= 0 && lq < Nb;
+      }
+      const int c = __popc(m);
+      int x = c;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+      }
+      if (Q < NIBZ) {
+        sBeg[Q] = base + x - c;
+        int p = base + x - c;
+        for (int sy = 0; sy < NS; sy++)
+          if (m >> sy & 1u) sSym[p++] = sy | (Q << 3);
+      }
+      const unsigned bal = __ballot_sync(0xffffffffu, mine);
+      if (mine) sQ[nq + __popc(bal & ((1u << lane) - 1u))] = Q;
+      nq += __popc(bal);
+      base += __shfl_sync(0xffffffffu, x, 31);
     }
-    sNp = np;
+    if (lane == 0) {
+      sBeg[NIBZ] = base;
+      sNq = nq;
+    }
   }
   __syncthreads();
-  const int r = blockIdx.z;
-  const size_t n2 = (size_t)Nz * Nz;
-  const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= n2) return;
-  const int i = (int)(e % Nz), j = (int)(e / Nz);
-  const int li = i / Nf, ni = i % Nf, lj = j / Nf, nj = j % Nf;
-  // per symmetry: offset of the permuted entry and its sign
-  long long off[NS];
-  double fac[NS];
-#pragma unroll
-  for (int sy = 0; sy < NS; sy++) {
-    off[sy] = (long long)(sL[sy + NS * li] * Nf + ni) + (long long)Nz * (sL[sy + NS * lj] * Nf + nj);
-    fac[sy] = sF[sy + NS * li] * sF[sy + NS * lj];
+  for (int t = threadIdx.x; t < npairs * NR; t += blockDim.x) {
+    const int p = t / NR, R = t % NR;
+    const int sy = sSym[p] & 7, Q = sSym[p] >> 3;
+    sE[t] = expSqR[Q + (size_t)NIBZ * (R + (size_t)NR * sy)];
   }
-  cplx acc[8];
+  const int nq = sNq;
+
+  // this thread's outputs: pair p, permuted-pair offsets and signs per symmetry
+  const int p = threadIdx.x / SUB, c = threadIdx.x % SUB;
+  const bool active = p < nl2;
+  unsigned offpk[NS / 2] = {0u, 0u, 0u, 0u};
+  unsigned negmask = 0u;
+  if (active) {
+    const int li = p % Nl, lj = p / Nl;
 #pragma unroll
-  for (int R = 0; R < 8; R++) acc[R] = cmk(0.0, 0.0);
-  const cplx* G = P.G[r];
-  const int np = sNp;
-  constexpr int U = 4;
-  for (int p0 = 0; p0 < np; p0 += U) {
-    cplx v[U];
-    int pr[U];
+    for (int sy = 0; sy < NS; sy++) {
+      const unsigned o = (unsigned)((lsym[sy + NS * li] + Nl * lsym[sy + NS * lj]) * PH_TI + c);
+      offpk[sy >> 1] |= o << (16 * (sy & 1));
+      if (lfac[sy + NS * li] * lfac[sy + NS * lj] < 0.0) negmask |= 1u << sy;
+    }
+  }
+  cplx acc[OPT][NR];
 #pragma unroll
-    for (int u = 0; u < U; u++) {
-      pr[u] = p0 + u < np ? sPair[p0 + u] : -1;
-      v[u] = cmk(0.0, 0.0);
-      if (pr[u] >= 0) {
-        const int sy = pr[u] % NS, Q = pr[u] / NS;
-        long long o = off[0];
+  for (int k = 0; k < OPT; k++)
 #pragma unroll
-        for (int t = 1; t < NS; t++)
-          if (t == sy) o = off[t];
-        v[u] = __ldg(G + o + (long long)n2 * (Q * nh + w - slot0));
+    for (int R = 0; R < NR; R++) acc[k][R] = cmk(0.0, 0.0);
+
+  const size_t n2 = (size_t)Nz * Nz;
+  // constant indices keep the parameter struct out of local memory
+  const cplx* G = r == 0 ? P.G[0] : r == 1 ? P.G[1] : r == 2 ? P.G[2] : P.G[3];
+  const int stage_elems = nl2 * PH_TI;
+  const cplx* Gw = G + (size_t)Nz * nj;  // element (0, (0, nj)); column (b, nj) is Nz Nf b further
+  if (nq > 0) ph_stage(sPhi, Gw + n2 * (size_t)(sQ[0] * nh + w - slot0), stage_elems, Nl, Nf, Nz, ni0);
+  asm volatile("cp.async.commit_group;\n" ::);
+  for (int qi = 0; qi < nq; qi++) {
+    if (qi + 1 < nq)
+      ph_stage(sPhi + (size_t)((qi + 1) & 1) * stage_elems, Gw + n2 * (size_t)(sQ[qi + 1] * nh + w - slot0),
+               stage_elems, Nl, Nf, Nz, ni0);
+    asm volatile("cp.async.commit_group;\n" ::);
+    asm volatile("cp.async.wait_group 1;\n" ::);
+    __syncthreads();
+    const cplx* S = sPhi + (size_t)(qi & 1) * stage_elems;
+    const int Q = sQ[qi];
+    const int pe = sBeg[Q + 1];
+    for (int pp = sBeg[Q]; pp < pe; pp++) {
+      const int sy = sSym[pp] & 7;
+      cplx e[NR];
+#pragma unroll
+      for (int R = 0; R < NR; R++) e[R] = sE[pp * NR + R];
+      if (active) {
+        const unsigned wpk = sy < 4 ? (sy < 2 ? offpk[0] : offpk[1]) : (sy < 6 ? offpk[2] : offpk[3]);
+        const unsigned off = (sy & 1) ? wpk >> 16 : wpk & 0xffffu;
+        const unsigned neg = negmask >> sy & 1u;
+#pragma unroll
+        for (int k = 0; k < OPT; k++) {
+          cplx v = S[off + SUB * k];
+          v.x = ph_sign(v.x, neg);
+          v.y = ph_sign(v.y, neg);
+#pragma unroll
+          for (int R = 0; R < NR; R++) acc[k][R] = cfma(v, e[R], acc[k][R]);
+        }
       }
     }
-#pragma unroll
-    for (int u = 0; u < U; u++) {
-      if (pr[u] < 0) continue;
-      const int sy = pr[u] % NS, Q = pr[u] / NS;
-      double f = fac[0];
-#pragma unroll
-      for (int t = 1; t < NS; t++)
-        if (t == sy) f = fac[t];
-      const cplx vv = cscale(v[u], f);
-      const cplx* eq = sE + Q + (size_t)NIBZ * NR * sy;
-#pragma unroll
-      for (int R = 0; R < 8; R++)
-        if (R < NR) acc[R] = cfma(vv, eq[(size_t)NIBZ * R], acc[R]);
-    }
+    __syncthreads();
   }
-  cplx* out = P.PhiR[r];
-  for (int R = 0; R < NR; R++) out[e + n2 * ((size_t)w + (size_t)nh * R)] = cscale(acc[R], inv_nx);
+  asm volatile("cp.async.wait_group 0;\n" ::);
+  if (!active) return;
+  const int li = p % Nl, lj = p / Nl;
+  cplx* out = r == 0 ? P.PhiR[0] : r == 1 ? P.PhiR[1] : r == 2 ? P.PhiR[2] : P.PhiR[3];
+#pragma unroll
+  for (int k = 0; k < OPT; k++) {
+    const int ni = ni0 + c + SUB * k;
+    if (ni >= Nf) continue;
+    const size_t e = (size_t)(li * Nf + ni) + (size_t)Nz * (lj * Nf + nj);
+#pragma unroll
+    for (int R = 0; R < NR; R++) out[e + n2 * ((size_t)w + (size_t)nh * R)] = cscale(acc[k][R], inv_nx);
+  }
 }
 
 // Crossing tensors per IBZ momentum Q; layout (Nl^4, NIBZ, NR) with l1 fastest.
@@ -165,6 +260,53 @@ __global__ void k_M(cplx* __restrict__ M, int which, const double* __restrict__ 
   M[e] = out;
 }
 
+// k_phir instantiations by outputs per thread (OPT) and NR; every candidate
+// forms each output's sum in the same order, so all write the same bits.
+typedef void (*PhirFn)(PhirPtrs, const cplx*, const int*, const int*, const double*, int, int, int, int, int, int,
+                       int, double);
+struct PhirCand {
+  const char* name;
+  int opt;
+  PhirFn fn1, fn4, fn6;
+};
+static const PhirCand kPhirCands[] = {
+    {"opt2", 2, k_phir<2, 1>, k_phir<2, 4>, k_phir<2, 6>},
+    {"opt4", 4, k_phir<4, 1>, k_phir<4, 4>, k_phir<4, 6>},
+    {"opt1", 1, k_phir<1, 1>, k_phir<1, 4>, k_phir<1, 6>},
+};
+constexpr int kNumPhirCands = sizeof(kPhirCands) / sizeof(kPhirCands[0]);
+
+static int phir_threads(const tups_ctx* ctx, int cand) {
+  const int opt = kPhirCands[cand].opt;
+  return (ctx->d.Nl * ctx->d.Nl * (PH_TI / opt) + 31) / 32 * 32;
+}
+
+static bool phir_fits(const tups_ctx* ctx, int cand) {
+  return phir_threads(ctx, cand) <= phir_max_threads(kPhirCands[cand].opt, ctx->d.NR);
+}
+
+static int phir_run(tups_ctx* ctx, const PhirPtrs& P, int cand) {
+  const auto& d = ctx->d;
+  const PhirCand& C = kPhirCands[cand];
+  PhirFn fn = d.NR == 1 ? C.fn1 : d.NR == 4 ? C.fn4 : C.fn6;
+  int npairs = 0;
+  for (int v : ctx->symlist) npairs += v ? 1 : 0;
+  const int nl2 = d.Nl * d.Nl;
+  const int threads = phir_threads(ctx, cand);
+  if (!phir_fits(ctx, cand)) return set_error(ctx, TUPS_ERR_BADDIM, "k_phir: too many form-factor pairs for one CTA");
+  const size_t sm = (size_t)2 * nl2 * PH_TI * sizeof(cplx) + (size_t)npairs * d.NR * sizeof(cplx) +
+                    ((size_t)npairs + 2 * d.NIBZ + 1) * sizeof(int);
+  if (sm > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return cuda_check(ctx, e, "k_phir smem attribute");
+  }
+  const int ntile = (d.Nf + PH_TI - 1) / PH_TI;
+  dim3 grid(ntile * d.Nf, d.Nf / 2, 4);
+  fn<<<grid, threads, sm, ctx->stream>>>(P, ctx->t.expSqR, ctx->t.symlist, ctx->t.lsym, ctx->t.lfac, d.Nz, d.Nf,
+                                         d.Nl, d.NIBZ, npairs, ctx->slot0, d.Nb, 1.0 / d.Nx);
+  return after_launch(ctx, "k_phir");
+}
+
 int launch_phir(tups_ctx* ctx) {
   const auto& d = ctx->d;
   PhirPtrs P;
@@ -172,20 +314,33 @@ int launch_phir(tups_ctx* ctx) {
     P.G[r] = ctx->s.G[r];
     P.PhiR[r] = ctx->s.PhiR[r];
   }
-  if (d.NR > 8) return set_error(ctx, TUPS_ERR_BADDIM, "NR > 8 not supported");
+  if (d.NR != 1 && d.NR != 4 && d.NR != 6) return set_error(ctx, TUPS_ERR_BADDIM, "k_phir: NR not in {1, 4, 6}");
   if (d.Nl > 16) return set_error(ctx, TUPS_ERR_BADDIM, "Nl > 16 not supported by k_phir");
-  const size_t n2 = (size_t)d.Nz * d.Nz;
-  const size_t sm = (size_t)d.NIBZ * d.NR * NS * sizeof(cplx) + (size_t)d.NIBZ * NS * sizeof(int);
-  if (sm > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(k_phir, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (e != cudaSuccess) return cuda_check(ctx, e, "k_phir smem attribute");
+  // the tuner: Phi(R) is a pure function of Gamma and the tables, so the
+  // candidates run on the call's own operands
+  const std::string key = "k_phir Nl=" + std::to_string(d.Nl) + " Nf=" + std::to_string(d.Nf) +
+                          " NIBZ=" + std::to_string(d.NIBZ) + " Nb=" + std::to_string(d.Nb) +
+                          " slot0=" + std::to_string(ctx->slot0);
+  // the candidates whose CTA fits this Nl; the first one is the default
+  std::vector<int> fit;
+  std::vector<std::string> names;
+  for (int c = 0; c < kNumPhirCands; c++)
+    if (phir_fits(ctx, c)) {
+      fit.push_back(c);
+      names.push_back(kPhirCands[c].name);
+    }
+  if (fit.empty()) return set_error(ctx, TUPS_ERR_BADDIM, "k_phir: too many form-factor pairs for one CTA");
+  int choice = 0;
+  int rc = TUPS_OK;
+  if (ctx->autotune && !tune_get(key, &choice) && tune_allowed(ctx)) {
+    rc = tune_pick(ctx, key, (int)fit.size(), names, [&](int c) { return phir_run(ctx, P, fit[c]); }, 2, &choice);
+    if (rc) return rc;
   }
-  dim3 grid(cdiv(n2, 256), d.Nf / 2, 4);
-  k_phir<<<grid, 256, sm, ctx->stream>>>(P, ctx->t.expSqR, ctx->t.symlist, ctx->t.lsym, ctx->t.lfac, d.Nz, d.Nf,
-                                         d.Nl, d.NIBZ, d.NR, ctx->slot0, d.Nb, 1.0 / d.Nx);
-  int rc = after_launch(ctx, "k_phir");
+  if (choice < 0 || choice >= (int)fit.size()) choice = 0;
+  rc = phir_run(ctx, P, fit[choice]);
   if (rc) return rc;
   // a sharded context summed over its own momenta: Phi(R) over all ranks
+  const size_t n2 = (size_t)d.Nz * d.Nz;
   for (int r = 0; r < 4 && !rc; r++)
     rc = exchange(ctx, TUPS_XCH_PHIR + r, reinterpret_cast<double*>(ctx->s.PhiR[r]),
                   2 * n2 * (size_t)(d.Nf / 2) * d.NR, TUPS_XCH_SUM);
