@@ -603,7 +603,7 @@ def run_bse_batched(args):
     from tups_b200.bse_batched import algorithmic_flops, make_instances
     from oracle import lu as LU
     workers = min(16, os.cpu_count() or 1)
-    inst = make_instances(n_q=64, n_w=16, nf=64, seed=0, workers=workers)
+    inst = make_instances(n_q=args.lu_q, n_w=16, nf=64, seed=0, workers=workers)
     flops = algorithmic_flops(inst.n)
     # CPU sample: two instances of each size, LAPACK zgetrf/zgetrs on all host threads
     sample = []
@@ -794,6 +794,8 @@ def main():
     ap.add_argument("--slices", type=int, nargs="+", default=[2, 3, 4, 5, 6, 7, 8], help="zgemm_split: slice counts")
     ap.add_argument("--n-tile", type=int, nargs="+", default=[0],
                     help="zgemm_split: column tiles of the split GEMM to compare (0 = automatic)")
+    ap.add_argument("--lu-q", type=int, default=64,
+                    help="bse_lu_1024: momenta (x 16 frequencies = instances); fewer for a small profiling case")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-split", action="store_true", help="skip the split-precision iterations")
     ap.add_argument("--no-graph", action="store_true", help="launch the timed iterations kernel by kernel")

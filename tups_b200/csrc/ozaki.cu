@@ -23,6 +23,7 @@
 #include <cuda.h>
 
 #include <algorithm>
+#include <cstdio>
 #include <atomic>
 #include <cstring>
 
@@ -43,7 +44,9 @@ __device__ __forceinline__ const cplx* oz_part(const OzOperand& o, int part, int
   const bool bse = part == 1 ? o.bse1 : o.bse2;
   if (bse) {
     const int q = o.q_begin + inst / 4, r = inst % 4;
-    return o.F[r] + (size_t)o.Nz * o.Nz * q;
+    // constant indices keep the parameter struct out of local memory
+    const cplx* Fr = r == 0 ? o.F[0] : r == 1 ? o.F[1] : r == 2 ? o.F[2] : o.F[3];
+    return Fr + (size_t)o.Nz * o.Nz * q;
   }
   return part == 1 ? o.p1 + (size_t)o.s1 * inst : o.p2 + (size_t)o.s2 * inst;
 }
@@ -678,6 +681,13 @@ void oz_bind_work(OzRun& R, const OzWork& w, void* base) {
   R.acc = nullptr;
 }
 
+// a failed CUDA step of oz_run on stderr (the batched ZGEMM entry point has no
+// context to keep a message in)
+static int oz_fail(const char* step, cudaError_t e) {
+  std::fprintf(stderr, "tups split GEMM: %s failed: %s\n", step, e == cudaSuccess ? "-" : cudaGetErrorString(e));
+  return TUPS_ERR_CUDA;
+}
+
 int oz_run(OzRun& R, cudaStream_t stream, long long* launches) {
   const int M = R.M, N = R.N, s = R.s, batch = R.batch;
   if (s < 1 || s > 8) return TUPS_ERR_BADARG;
@@ -696,7 +706,7 @@ int oz_run(OzRun& R, cudaStream_t stream, long long* launches) {
     k_oz_split_cols<<<gc, 256, 0, stream>>>(R.B, N, s, Kpad, R.b_slices, R.cscale);
     if (launches) (*launches)++;
     cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return TUPS_ERR_CUDA;
+    if (e != cudaSuccess) return oz_fail("slice kernels launch", e);
   }
   OzGemm P;
   std::memset(&P, 0, sizeof(P));
@@ -733,11 +743,13 @@ int oz_run(OzRun& R, cudaStream_t stream, long long* launches) {
     P.stall_test = g_oz_stall_test.exchange(0);
   }
   CUtensorMap ta, tb;
-  if (!make_map(&ta, R.a_slices, (long long)batch * s * M, Kpad, OZ_BM)) return TUPS_ERR_CUDA;
-  if (!make_map(&tb, R.b_slices, (long long)batch * s * 2 * N, Kpad, P.n_tile)) return TUPS_ERR_CUDA;
+  if (!make_map(&ta, R.a_slices, (long long)batch * s * M, Kpad, OZ_BM))
+    return oz_fail("tensor map of the A slices", cudaSuccess);
+  if (!make_map(&tb, R.b_slices, (long long)batch * s * 2 * N, Kpad, P.n_tile))
+    return oz_fail("tensor map of the B slices", cudaSuccess);
   const size_t smem = oz_smem_bytes(P.n_tile);
   cudaError_t e = cudaFuncSetAttribute(k_oz_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return TUPS_ERR_CUDA;
+  if (e != cudaSuccess) return oz_fail("k_oz_gemm shared memory attribute", e);
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -745,7 +757,7 @@ int oz_run(OzRun& R, cudaStream_t stream, long long* launches) {
   k_oz_gemm<<<grid, OZ_THREADS2, smem, stream>>>(ta, tb, P);
   if (launches) (*launches)++;
   e = cudaGetLastError();
-  return e == cudaSuccess ? TUPS_OK : TUPS_ERR_CUDA;
+  return e == cudaSuccess ? TUPS_OK : oz_fail("k_oz_gemm launch", e);
 }
 
 }  // namespace tups
@@ -790,8 +802,9 @@ extern "C" int tups_zgemm_split(int batch, int M, int N, int K, const double* A,
   int rc = oz_run(R, st, nullptr);
   if (rc) return rc;
   double flag = 0.0;
-  if (cudaMemcpyAsync(&flag, status, sizeof(double), cudaMemcpyDeviceToHost, st) != cudaSuccess) return TUPS_ERR_CUDA;
-  if (cudaStreamSynchronize(st) != cudaSuccess) return TUPS_ERR_CUDA;
+  cudaError_t e = cudaMemcpyAsync(&flag, status, sizeof(double), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return oz_fail("split ZGEMM completion", e);
   return flag != 0.0 ? TUPS_ERR_TIMEOUT : TUPS_OK;
 }
 
