@@ -272,6 +272,8 @@ def run_tups(args, wl_name: str, wl: dict):
     peak64 = fp64_peak_tflops(device)
     params = Params(**{k: v for k, v in wl.items() if k in Params.__dataclass_fields__})
     sol = Solver(params, device=device)
+    if args.crossing_products:
+        sol.set_crossing_products(args.crossing_products)
     if args.bse_slices:
         sol.set_bse_precision(args.bse_slices)
     K, W = args.steps, args.warmup
@@ -796,6 +798,8 @@ def main():
                     help="zgemm_split: column tiles of the split GEMM to compare (0 = automatic)")
     ap.add_argument("--lu-q", type=int, default=64,
                     help="bse_lu_1024: momenta (x 16 frequencies = instances); fewer for a small profiling case")
+    ap.add_argument("--crossing-products", type=int, default=0, choices=[0, 3, 4],
+                    help="real tensor-core products per complex one in the crossing GEMM (0 = library default)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-split", action="store_true", help="skip the split-precision iterations")
     ap.add_argument("--no-graph", action="store_true", help="launch the timed iterations kernel by kernel")

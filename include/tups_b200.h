@@ -279,6 +279,12 @@ int tups_set_split_tile(int n_tile);
  * the choice.  Not run during a stream capture.  On by default; the
  * environment variable TUPS_AUTOTUNE=0 or enable = 0 fixes the default tiles. */
 int tups_set_autotune(tups_ctx* ctx, int enable);
+/* Real tensor-core products per complex multiply-add in the crossing GEMM of
+ * tups_calculate_PAE: 3 (default; Gauss: Xr Mr, Xi Mi, (Xr + Xi)(Mr + Mi))
+ * or 4, for 5 or more form factors.  Both agree with the reference's
+ * crossing sums (parquet_EQContribs.f90:44-524) to rounding; the three-product
+ * form rounds differently.  No counterpart in the reference. */
+int tups_set_crossing_products(tups_ctx* ctx, int products);
 /* The choices made so far in this process as text, one line per kernel and
  * shape: "<kernel> <shape> | choice <name> | <name>=<ms> ...".  Writes at
  * most len bytes (NUL-terminated) and returns the length the whole table

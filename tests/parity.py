@@ -138,11 +138,12 @@ def readout_side_by_side(p: O.Params, full_iterations: int = 2, device: int = 0)
     return errs
 
 
-def run_side_by_side(p: O.Params, iterations: int, device: int = 0):
+def run_side_by_side(p: O.Params, iterations: int, device: int = 0, crossing_products: int = 3):
     """Returns (errors per phase, oracle state, solver)."""
     from tups_b200 import Solver
     st = O.initialize(p)
     sol = Solver(to_solver_params(p), device=device)
+    sol.set_crossing_products(crossing_products)
     errs: dict = {}
     errs["init_F"] = [max(rel(sol.F(r), st.F[r]) for r in CH)]
     for ite in range(iterations):

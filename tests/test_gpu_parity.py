@@ -46,6 +46,19 @@ def test_phases_side_by_side(gpu_lib, case):
     sol.close()
 
 
+@pytest.mark.parametrize("case", [
+    dict(beta=2.0, U=2.0, nParticle=0.9, Nx=4, Nf=8, neighbours=2),
+    dict(beta=3.0, U=1.5, nParticle=0.95, Nx=8, Nf=8, neighbours=3, tprime=-0.2),
+], ids=["nl5", "nl9_tprime"])
+def test_four_product_crossing_side_by_side(gpu_lib, case):
+    """The crossing GEMM with four real products per complex one meets the
+    same per-phase bound as the three-product (Gauss) default."""
+    p = O.Params(f_damping=0.5, ite_max=10, **case)
+    errs, st, sol = parity.run_side_by_side(p, 3, crossing_products=4)
+    _check(errs)
+    sol.close()
+
+
 def test_tables_bit_exact(gpu_lib):
     from tups_b200 import Solver
     p = O.Params(Nx=8, Nf=8, neighbours=3)

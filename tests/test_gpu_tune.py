@@ -34,7 +34,7 @@ def test_tuned_tiles_equal_default_tiles(gpu_lib, case):
         assert np.array_equal(a[1][r], b[1][r]) and np.array_equal(a[2][r], b[2][r]), r
     table = tuning_table()
     keys = {ln.split(" | ")[0]: ln for ln in table}
-    pae = [k for k in keys if k.startswith(f"k_pae_mma Nl={Nl} Nf={p.Nf} ")]
+    pae = [k for k in keys if k.startswith((f"k_pae_mma Nl={Nl} Nf={p.Nf} ", f"k_pae_mma(3M) Nl={Nl} Nf={p.Nf} "))]
     bse = f"k_bse_gemm Nz={Nz}"
     assert pae and bse in keys, table
     for k in (pae[0], bse):

@@ -101,6 +101,7 @@ _PROTOS = {
     "tups_get_vertex_slots": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p],
     "tups_set_vertex_slots": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p],
     "tups_set_autotune": [C.c_void_p, C.c_int],
+    "tups_set_crossing_products": [C.c_void_p, C.c_int],
     "tups_set_split_wait": [C.c_longlong, C.c_int],
     "tups_set_split_tile": [C.c_int],
     "tups_bse_lu_split_batched": [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double),

@@ -490,6 +490,26 @@ static const PaeCand kPaeWide[] = {
     {"flat_bn96_tn6", run_pae<6, 2, 4, 2, 0>, 96},
     {"flat_bn112_tn7", run_pae<7, 2, 4, 2, 0>, 112},
 };
+// three real products per complex one (Gauss): a different rounding of each
+// sum, so these form their own candidate set, chosen by the context's
+// crossing-products setting; the widths that fit 128 registers unspilled
+// (index 0: the tuner's pick on a B200 at 8x8 / Nl = 5, 1.560 ms against
+// 1.573 for 64 columns; at 16x16 / Nl = 9 64 columns won, 372 ms against
+// 392 for 48); three-stage pipelines at the widths that keep two CTAs per SM
+static const PaeCand kPaeNl5G3[] = {
+    {"g3_flat_bn32_tn2", run_pae<2, 2, 4, 2, 0, true>, 32},
+    {"g3_flat_bn64_tn4", run_pae<4, 2, 4, 2, 0, true>, 64},
+    {"g3_flat_bn48_tn3", run_pae<3, 2, 4, 2, 0, true>, 48},
+    {"g3_flat_bn32_tn2_s3", run_pae<2, 2, 4, 3, 0, true>, 32},
+    {"g3_flat_bn48_tn3_s3", run_pae<3, 2, 4, 3, 0, true>, 48},
+};
+static const PaeCand kPaeWideG3[] = {
+    {"g3_flat_bn64_tn4", run_pae<4, 2, 4, 2, 0, true>, 64},
+    {"g3_flat_bn48_tn3", run_pae<3, 2, 4, 2, 0, true>, 48},
+    {"g3_flat_bn32_tn2", run_pae<2, 2, 4, 2, 0, true>, 32},
+    {"g3_flat_bn48_tn3_s3", run_pae<3, 2, 4, 3, 0, true>, 48},
+    {"g3_flat_bn32_tn2_s3", run_pae<2, 2, 4, 3, 0, true>, 32},
+};
 
 static int pae_all(tups_ctx* ctx, const PaePtrs& P, const PaeCand& c) {
   const auto& d = ctx->d;
@@ -521,11 +541,15 @@ int launch_pae(tups_ctx* ctx) {
   }
   // F = Phi + Lambda Nc, then the diagonal family, then the anti-diagonal one
   const int nl2 = d.Nl * d.Nl;
-  const PaeCand* cands = nl2 <= 8 ? kPaeNl1 : nl2 <= 32 ? kPaeNl5 : kPaeWide;
+  const bool g3 = ctx->pae_products == 3 && nl2 > 8;
+  const PaeCand* cands = nl2 <= 8 ? kPaeNl1 : nl2 <= 32 ? (g3 ? kPaeNl5G3 : kPaeNl5) : (g3 ? kPaeWideG3 : kPaeWide);
   const int n_cand = nl2 <= 8 ? (int)(sizeof(kPaeNl1) / sizeof(PaeCand))
-                     : nl2 <= 32 ? (int)(sizeof(kPaeNl5) / sizeof(PaeCand))
-                                 : (int)(sizeof(kPaeWide) / sizeof(PaeCand));
-  const std::string key = "k_pae_mma Nl=" + std::to_string(d.Nl) + " Nf=" + std::to_string(d.Nf) +
+                     : nl2 <= 32 ? (g3 ? (int)(sizeof(kPaeNl5G3) / sizeof(PaeCand))
+                                       : (int)(sizeof(kPaeNl5) / sizeof(PaeCand)))
+                                 : (g3 ? (int)(sizeof(kPaeWideG3) / sizeof(PaeCand))
+                                       : (int)(sizeof(kPaeWide) / sizeof(PaeCand)));
+  const std::string key = std::string(g3 ? "k_pae_mma(3M)" : "k_pae_mma") + " Nl=" + std::to_string(d.Nl) +
+                          " Nf=" + std::to_string(d.Nf) +
                           " NIBZ=" + std::to_string(d.NIBZ) + " NR=" + std::to_string(d.NR) +
                           " Nb=" + std::to_string(d.Nb) + " slot0=" + std::to_string(ctx->slot0);
   int choice = 0;
@@ -541,3 +565,20 @@ int launch_pae(tups_ctx* ctx) {
 }
 
 }  // namespace tups
+
+// Real DMMA products per complex one in the crossing GEMM: 3 (default;
+// Gauss: Xr Mr, Xi Mi, (Xr + Xi)(Mr + Mi)) or 4.  Both agree with the reference
+// to rounding; the three-product form rounds differently.
+extern "C" int tups_set_crossing_products(tups_ctx* ctx, int products) {
+  if (!ctx || (products != 3 && products != 4)) return TUPS_ERR_BADARG;
+  if (products != ctx->pae_products) {
+    // iterations captured as CUDA graphs hold the other form's kernels
+    for (auto& g : ctx->graph_exec)
+      if (g) {
+        cudaGraphExecDestroy(g);
+        g = nullptr;
+      }
+  }
+  ctx->pae_products = products;
+  return TUPS_OK;
+}

@@ -154,25 +154,24 @@ __global__ void __launch_bounds__(256) k_sde_sigma(const cplx* __restrict__ Gkw,
 __global__ void k_symmetrize(const cplx* __restrict__ SigmaV, const cplx* __restrict__ order2,
                              const int* __restrict__ ibz, const int* __restrict__ symlist, const int* __restrict__ symq,
                              cplx* __restrict__ Sigma, int Nx, int Ny, int Nf, int nxibz, int use_U2) {
-  const int nu = blockIdx.x * blockDim.x + threadIdx.x;
-  if (nu >= Nf) return;
-  for (int k = 0; k < Nx * Ny; k++) Sigma[(size_t)k * Nf + nu] = cmk(0.0, 0.0);
+  // one thread per output (k, nu): the sum, in the reference's (ip, s) loop
+  // order, of the IBZ values whose star images land on k (one per k on an
+  // even lattice), plus the U^2 term
+  const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (size_t)Nx * Ny * Nf) return;
+  const int nu = (int)(e % Nf), k = (int)(e / Nf);
+  const int kx = k / Ny + 1, ky = k % Ny + 1;
+  cplx acc = cmk(0.0, 0.0);
   int ip = 0;
   for (int qx = 1; qx <= nxibz; qx++)
-    for (int qy = 1; qy <= qx; qy++, ip++) {
-      const cplx v = SigmaV[(size_t)ip * Nf + nu];
+    for (int qy = 1; qy <= qx; qy++, ip++)
       for (int s = 0; s < NS; s++) {
         if (!symlist[NS * ip + s]) continue;
-        const int sx = symq[2 * (NS * ip + s)], sy = symq[2 * (NS * ip + s) + 1];
-        const size_t o = ((size_t)(sx - 1) * Ny + sy - 1) * Nf + nu;
-        Sigma[o] = cadd(Sigma[o], v);
+        if (symq[2 * (NS * ip + s)] == kx && symq[2 * (NS * ip + s) + 1] == ky)
+          acc = cadd(acc, SigmaV[(size_t)ip * Nf + nu]);
       }
-    }
-  if (use_U2)
-    for (int k = 0; k < Nx * Ny; k++) {
-      const size_t o = (size_t)k * Nf + nu;
-      Sigma[o] = cadd(Sigma[o], order2[o]);
-    }
+  if (use_U2) acc = cadd(acc, order2[e]);
+  Sigma[e] = acc;
   (void)ibz;
 }
 
@@ -290,7 +289,7 @@ int launch_sde(tups_ctx* ctx) {
                                                                             d.Ngrain, d.Nf, ctx->p.beta);
     if ((rc = after_launch(ctx, "k_nfourier"))) return rc;
   }
-  k_symmetrize<<<cdiv(d.Nf, 64), 64, 0, ctx->stream>>>(ctx->s.SigmaV, ctx->s.order2, ctx->t.ibz, ctx->t.symlist,
+  k_symmetrize<<<cdiv((long long)d.Nc * d.Nf, 128), 128, 0, ctx->stream>>>(ctx->s.SigmaV, ctx->s.order2, ctx->t.ibz, ctx->t.symlist,
                                                        ctx->t.symq, ctx->s.Sigma, d.Nx, d.Ny, d.Nf, d.Nx_IBZ,
                                                        ctx->p.use_U2);
   return after_launch(ctx, "k_symmetrize");

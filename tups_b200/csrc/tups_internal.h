@@ -151,6 +151,7 @@ struct tups_ctx {
   // tile-shape tuner (tune.cu): on by default, TUPS_AUTOTUNE=0 turns it off;
   // tile_tunings counts the tunings run by this context
   bool autotune = true;
+  int pae_products = 3;        // real DMMA products per complex one in the crossing GEMM (3 or 4)
   long long tile_tunings = 0;
   cudaGraphExec_t graph_exec[18] = {};
   long long graph_launches[18] = {};

@@ -292,6 +292,10 @@ class Solver:
         """Tile-shape tuner on (default) or off (fixed default tiles)."""
         self._call("tups_set_autotune", int(bool(enable)))
 
+    def set_crossing_products(self, products: int = 3) -> None:
+        """Real tensor-core products per complex one in the crossing GEMM: 3 (default) or 4."""
+        self._call("tups_set_crossing_products", int(products))
+
     # -- split-precision BSE --
     def set_bse_precision(self, slices: int = 0, ladder: bool = False) -> None:
         """slices = 0: FP64 tensor cores; 2..8: int8 slices per operand;
