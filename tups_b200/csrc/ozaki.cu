@@ -78,25 +78,35 @@ __device__ __forceinline__ cplx oz_b(const OzLine& v, int k, int j) {
   return k < v.K1 ? v.p1[k + (size_t)v.ld1 * j] : v.p2[(k - v.K1) + (size_t)v.ld2 * j];
 }
 
-// s int8 slices of v * 2^-e into out[i * slice_stride], |v 2^-e| < 1
-__device__ __forceinline__ void oz_cut(double v, int e, int s, int8_t* out, size_t slice_stride) {
-  double r = ldexp(v, -e);
-  for (int i = 0; i < s; i++) {
-    const double x = r * 128.0;
-    const double a = trunc(x);
-    out[i * slice_stride] = (int8_t)(int)a;
-    r = x - a;
-  }
-}
-
 __device__ __forceinline__ int oz_exponent(double maxabs) {
   int e = 0;
   if (maxabs > 0.0) frexp(maxabs, &e);
   return e;
 }
 
+// The s int8 slices of v 2^-e (|v 2^-e| < 1) are the base-128 digits, most
+// significant first and carrying the sign of v, of t = trunc(v 2^(7s - e)):
+// the same bytes as the repeated a = trunc(128 r), r = 128 r - a of the
+// error-free splitting (all steps exact in FP64), with
+// one scaling and one conversion instead of 4 s FP64 operations.  |t| <
+// 2^(7s) <= 2^56, so t is an exact int64.
+__device__ __forceinline__ long long oz_fixed(double v, int e, int s) {
+  return __double2ll_rz(ldexp(v, OZ_SLICE_BITS * s - e));
+}
+// digit i (0 = most significant) of t as a byte
+__device__ __forceinline__ uint32_t oz_digit(long long t, int i, int s) {
+  const long long u = t < 0 ? -t : t;
+  const int d = (int)((u >> (OZ_SLICE_BITS * (s - 1 - i))) & 127);
+  return (uint32_t)(uint8_t)(int8_t)(t < 0 ? -d : d);
+}
+
 // Rows of A': one CTA per 32 rows of one instance.  out: [inst][s][M][Kpad].
-__global__ void __launch_bounds__(256) k_oz_split_rows(OzOperand A, int M, int s, int Kpad, int8_t* __restrict__ out,
+// Pass 1 finds each row's scale (a warp per 8 columns at a time, four loads
+// in flight per thread); pass 2 stages 32 x 64 complex tiles in shared
+// memory (eight loads in flight per thread) and writes each row's slices as
+// 8-byte runs.
+constexpr int OZ_RT = 64;  // columns per staged tile of the row slicer
+__global__ void __launch_bounds__(256, 3) k_oz_split_rows(OzOperand A, int M, int s, int Kpad, int8_t* __restrict__ out,
                                                        double* __restrict__ rscale) {
   const int inst = blockIdx.y;
   const int m0 = blockIdx.x * 32;
@@ -104,17 +114,26 @@ __global__ void __launch_bounds__(256) k_oz_split_rows(OzOperand A, int M, int s
   const OzLine V = oz_view(A, inst);
   __shared__ double smax[8][33];
   __shared__ int sexp[32];
-  __shared__ cplx tile[32][33];
+  __shared__ cplx tile[OZ_RT][33];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   {
     const int m = m0 + lane;
-    double mx = 0.0;
-    if (m < M)
-      for (int k = w; k < Kc; k += 8) {
-        const cplx v = oz_a(V, m, k);
-        mx = fmax(mx, fmax(fabs(v.x), fabs(v.y)));
+    double mx0 = 0.0, mx1 = 0.0, mx2 = 0.0, mx3 = 0.0;
+    if (m < M) {
+      int k = w;
+      for (; k + 24 < Kc; k += 32) {
+        const cplx v0 = oz_a(V, m, k), v1 = oz_a(V, m, k + 8), v2 = oz_a(V, m, k + 16), v3 = oz_a(V, m, k + 24);
+        mx0 = fmax(mx0, fmax(fabs(v0.x), fabs(v0.y)));
+        mx1 = fmax(mx1, fmax(fabs(v1.x), fabs(v1.y)));
+        mx2 = fmax(mx2, fmax(fabs(v2.x), fabs(v2.y)));
+        mx3 = fmax(mx3, fmax(fabs(v3.x), fabs(v3.y)));
       }
-    smax[w][lane] = mx;
+      for (; k < Kc; k += 8) {
+        const cplx v = oz_a(V, m, k);
+        mx0 = fmax(mx0, fmax(fabs(v.x), fabs(v.y)));
+      }
+    }
+    smax[w][lane] = fmax(fmax(mx0, mx1), fmax(mx2, mx3));
   }
   __syncthreads();
   if (threadIdx.x < 32) {
@@ -128,38 +147,63 @@ __global__ void __launch_bounds__(256) k_oz_split_rows(OzOperand A, int M, int s
   __syncthreads();
   const size_t slice_stride = (size_t)M * Kpad;
   int8_t* base = out + (size_t)inst * s * slice_stride;
-  // thread -> (row, group of 4 columns): 8 groups x 32 rows
+  // thread -> (row rr, 8 consecutive columns 8 cg .. 8 cg + 7): 8 groups x 32 rows
   const int cg = threadIdx.x & 7, rr = threadIdx.x >> 3;
-  for (int k0 = 0; k0 < Kc; k0 += 32) {
-    // load a 32 x 32 tile, rows fastest
-    for (int e = threadIdx.x; e < 32 * 32; e += 256) {
-      const int r = e & 31, c = e >> 5;
-      const int m = m0 + r, k = k0 + c;
-      cplx v = cmk(0.0, 0.0);
-      if (m < M && k < Kc) v = oz_a(V, m, k);
-      tile[c][r] = v;
+  const int m = m0 + rr;
+  const int e = sexp[rr];
+  const bool vec = (Kc & 7) == 0;
+  for (int k0 = 0; k0 < Kc; k0 += OZ_RT) {
+    // load a 32 x 64 tile, rows fastest: eight independent loads per thread
+    cplx v[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+      const int x = threadIdx.x + 256 * j;
+      const int r = x & 31, c = x >> 5;
+      const int mm = m0 + r, k = k0 + c;
+      v[j] = (mm < M && k < Kc) ? oz_a(V, mm, k) : cmk(0.0, 0.0);
+    }
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+      const int x = threadIdx.x + 256 * j;
+      tile[x >> 5][x & 31] = v[j];
     }
     __syncthreads();
-    const int m = m0 + rr;
-    const int k = k0 + cg * 4;
+    const int k = k0 + cg * 8;
     if (m < M && k < Kc) {
-      const int e = sexp[rr];
-      int8_t re[4][8], im[4][8];
-      for (int c = 0; c < 4; c++) {
-        const cplx v = (k + c < Kc) ? tile[cg * 4 + c][rr] : cmk(0.0, 0.0);
-        oz_cut(v.x, e, s, &re[c][0], 1);
-        oz_cut(v.y, e, s, &im[c][0], 1);
+      uint32_t lre[8], hre[8], lim[8], him[8];
+#pragma unroll
+      for (int i = 0; i < 8; i++) lre[i] = hre[i] = lim[i] = him[i] = 0u;
+      // column c = (j + cg) & 7 at step j: the eight lanes of a quarter warp
+      // (cg = 0..7, one row) then read eight different banks
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        const int c = (j + cg) & 7;
+        const cplx x = (k + c < Kc) ? tile[cg * 8 + c][rr] : cmk(0.0, 0.0);
+        const long long tr = oz_fixed(x.x, e, s), ti = oz_fixed(x.y, e, s);
+        const int sh = 8 * (c & 3);
+        const bool lo = c < 4;
+#pragma unroll
+        for (int i = 0; i < 8; i++)
+          if (i < s) {
+            const uint32_t dr = oz_digit(tr, i, s) << sh, di = oz_digit(ti, i, s) << sh;
+            lre[i] |= lo ? dr : 0u;
+            hre[i] |= lo ? 0u : dr;
+            lim[i] |= lo ? di : 0u;
+            him[i] |= lo ? 0u : di;
+          }
       }
       int8_t* row = base + (size_t)m * Kpad;
-      for (int i = 0; i < s; i++) {
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+        if (i >= s) continue;
         int8_t* dst = row + (size_t)i * slice_stride;
-        if ((Kc & 3) == 0 && k + 3 < Kc) {
-          *reinterpret_cast<char4*>(dst + k) = make_char4(re[0][i], re[1][i], re[2][i], re[3][i]);
-          *reinterpret_cast<char4*>(dst + Kc + k) = make_char4(im[0][i], im[1][i], im[2][i], im[3][i]);
+        if (vec && k + 7 < Kc) {
+          *reinterpret_cast<uint2*>(dst + k) = make_uint2(lre[i], hre[i]);
+          *reinterpret_cast<uint2*>(dst + Kc + k) = make_uint2(lim[i], him[i]);
         } else {
-          for (int c = 0; c < 4 && k + c < Kc; c++) {
-            dst[k + c] = re[c][i];
-            dst[Kc + k + c] = im[c][i];
+          for (int c = 0; c < 8 && k + c < Kc; c++) {
+            dst[k + c] = (int8_t)((c < 4 ? lre[i] : hre[i]) >> (8 * (c & 3)));
+            dst[Kc + k + c] = (int8_t)((c < 4 ? lim[i] : him[i]) >> (8 * (c & 3)));
           }
         }
       }
@@ -168,15 +212,16 @@ __global__ void __launch_bounds__(256) k_oz_split_rows(OzOperand A, int M, int s
   }
   // zero the K padding [2 Kc, Kpad) of this CTA's rows
   const int pad = Kpad - 2 * Kc;
-  for (int e = threadIdx.x; e < 32 * pad * s; e += 256) {
-    const int b = e % pad, r = (e / pad) % 32, i = e / (pad * 32);
+  for (int x = threadIdx.x; x < 32 * pad * s; x += 256) {
+    const int b = x % pad, r = (x / pad) % 32, i = x / (pad * 32);
     if (m0 + r < M) base[(size_t)i * slice_stride + (size_t)(m0 + r) * Kpad + 2 * Kc + b] = 0;
   }
 }
 
 // Columns of B': one warp per complex column j of B (K1 + K2 long); writes
-// rows 2j and 2j+1 of every slice.  out: [inst][s][2N][Kpad].
-__global__ void __launch_bounds__(256) k_oz_split_cols(OzOperand B, int N, int s, int Kpad, int8_t* __restrict__ out,
+// rows 2j and 2j+1 of every slice.  out: [inst][s][2N][Kpad].  The column
+// is read twice (scale, then slices); the second read hits L1.
+__global__ void __launch_bounds__(256, 4) k_oz_split_cols(OzOperand B, int N, int s, int Kpad, int8_t* __restrict__ out,
                                                        double* __restrict__ cscale) {
   const int inst = blockIdx.y;
   const int j = blockIdx.x * 8 + (threadIdx.x >> 5);
@@ -184,39 +229,63 @@ __global__ void __launch_bounds__(256) k_oz_split_cols(OzOperand B, int N, int s
   if (j >= N) return;
   const int Kc = B.K1 + B.K2;
   const OzLine V = oz_view(B, inst);
-  double mx = 0.0;
-  for (int k = lane; k < Kc; k += 32) {
-    const cplx v = oz_b(V, k, j);
-    mx = fmax(mx, fmax(fabs(v.x), fabs(v.y)));
+  double mx0 = 0.0, mx1 = 0.0, mx2 = 0.0, mx3 = 0.0;
+  {
+    int k = lane;
+    for (; k + 96 < Kc; k += 128) {
+      const cplx v0 = oz_b(V, k, j), v1 = oz_b(V, k + 32, j), v2 = oz_b(V, k + 64, j), v3 = oz_b(V, k + 96, j);
+      mx0 = fmax(mx0, fmax(fabs(v0.x), fabs(v0.y)));
+      mx1 = fmax(mx1, fmax(fabs(v1.x), fabs(v1.y)));
+      mx2 = fmax(mx2, fmax(fabs(v2.x), fabs(v2.y)));
+      mx3 = fmax(mx3, fmax(fabs(v3.x), fabs(v3.y)));
+    }
+    for (; k < Kc; k += 32) {
+      const cplx v = oz_b(V, k, j);
+      mx0 = fmax(mx0, fmax(fabs(v.x), fabs(v.y)));
+    }
   }
-  mx = warp_max(mx);
+  const double mx = warp_max(fmax(fmax(mx0, mx1), fmax(mx2, mx3)));
   const int e = oz_exponent(mx);
   if (lane == 0) cscale[(size_t)inst * N + j] = ldexp(1.0, e);
   const size_t slice_stride = (size_t)2 * N * Kpad;
   int8_t* r0 = out + (size_t)inst * s * slice_stride + (size_t)(2 * j) * Kpad;
   int8_t* r1 = r0 + Kpad;
+  const bool vec = (Kc & 3) == 0;
   for (int k = lane * 4; k < Kc; k += 128) {
-    int8_t re[4][8], im[4][8];
+    cplx v[4];
+#pragma unroll
+    for (int c = 0; c < 4; c++) v[c] = k + c < Kc ? oz_b(V, k + c, j) : cmk(0.0, 0.0);
+    uint32_t wre[8], wim[8], wnim[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) wre[i] = wim[i] = wnim[i] = 0u;
+#pragma unroll
     for (int c = 0; c < 4; c++) {
-      const cplx v = k + c < Kc ? oz_b(V, k + c, j) : cmk(0.0, 0.0);
-      oz_cut(v.x, e, s, &re[c][0], 1);
-      oz_cut(v.y, e, s, &im[c][0], 1);
+      const long long tr = oz_fixed(v[c].x, e, s), ti = oz_fixed(v[c].y, e, s);
+#pragma unroll
+      for (int i = 0; i < 8; i++)
+        if (i < s) {
+          wre[i] |= oz_digit(tr, i, s) << (8 * c);
+          wim[i] |= oz_digit(ti, i, s) << (8 * c);
+          // the slices of -Im are the negated slices of Im (truncation is odd)
+          wnim[i] |= oz_digit(-ti, i, s) << (8 * c);
+        }
     }
-    // the slices of -Im are the negated slices of Im (truncation is odd)
-    for (int i = 0; i < s; i++) {
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      if (i >= s) continue;
       int8_t* d0 = r0 + (size_t)i * slice_stride;
       int8_t* d1 = r1 + (size_t)i * slice_stride;
-      if ((Kc & 3) == 0 && k + 3 < Kc) {
-        *reinterpret_cast<char4*>(d0 + k) = make_char4(re[0][i], re[1][i], re[2][i], re[3][i]);
-        *reinterpret_cast<char4*>(d0 + Kc + k) = make_char4(-im[0][i], -im[1][i], -im[2][i], -im[3][i]);
-        *reinterpret_cast<char4*>(d1 + k) = make_char4(im[0][i], im[1][i], im[2][i], im[3][i]);
-        *reinterpret_cast<char4*>(d1 + Kc + k) = make_char4(re[0][i], re[1][i], re[2][i], re[3][i]);
+      if (vec && k + 3 < Kc) {
+        *reinterpret_cast<uint32_t*>(d0 + k) = wre[i];
+        *reinterpret_cast<uint32_t*>(d0 + Kc + k) = wnim[i];
+        *reinterpret_cast<uint32_t*>(d1 + k) = wim[i];
+        *reinterpret_cast<uint32_t*>(d1 + Kc + k) = wre[i];
       } else {
         for (int c = 0; c < 4 && k + c < Kc; c++) {
-          d0[k + c] = re[c][i];
-          d0[Kc + k + c] = (int8_t)(-im[c][i]);
-          d1[k + c] = im[c][i];
-          d1[Kc + k + c] = re[c][i];
+          d0[k + c] = (int8_t)(wre[i] >> (8 * c));
+          d0[Kc + k + c] = (int8_t)(wnim[i] >> (8 * c));
+          d1[k + c] = (int8_t)(wim[i] >> (8 * c));
+          d1[Kc + k + c] = (int8_t)(wre[i] >> (8 * c));
         }
       }
     }
