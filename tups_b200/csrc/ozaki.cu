@@ -221,7 +221,7 @@ __global__ void __launch_bounds__(256, 3) k_oz_split_rows(OzOperand A, int M, in
 // Columns of B': one warp per complex column j of B (K1 + K2 long); writes
 // rows 2j and 2j+1 of every slice.  out: [inst][s][2N][Kpad].  The column
 // is read twice (scale, then slices); the second read hits L1.
-__global__ void __launch_bounds__(256, 4) k_oz_split_cols(OzOperand B, int N, int s, int Kpad, int8_t* __restrict__ out,
+__global__ void __launch_bounds__(256) k_oz_split_cols(OzOperand B, int N, int s, int Kpad, int8_t* __restrict__ out,
                                                        double* __restrict__ cscale) {
   const int inst = blockIdx.y;
   const int j = blockIdx.x * 8 + (threadIdx.x >> 5);
@@ -255,9 +255,9 @@ __global__ void __launch_bounds__(256, 4) k_oz_split_cols(OzOperand B, int N, in
     cplx v[4];
 #pragma unroll
     for (int c = 0; c < 4; c++) v[c] = k + c < Kc ? oz_b(V, k + c, j) : cmk(0.0, 0.0);
-    uint32_t wre[8], wim[8], wnim[8];
+    uint32_t wre[8], wim[8];
 #pragma unroll
-    for (int i = 0; i < 8; i++) wre[i] = wim[i] = wnim[i] = 0u;
+    for (int i = 0; i < 8; i++) wre[i] = wim[i] = 0u;
 #pragma unroll
     for (int c = 0; c < 4; c++) {
       const long long tr = oz_fixed(v[c].x, e, s), ti = oz_fixed(v[c].y, e, s);
@@ -266,8 +266,6 @@ __global__ void __launch_bounds__(256, 4) k_oz_split_cols(OzOperand B, int N, in
         if (i < s) {
           wre[i] |= oz_digit(tr, i, s) << (8 * c);
           wim[i] |= oz_digit(ti, i, s) << (8 * c);
-          // the slices of -Im are the negated slices of Im (truncation is odd)
-          wnim[i] |= oz_digit(-ti, i, s) << (8 * c);
         }
     }
 #pragma unroll
@@ -275,15 +273,18 @@ __global__ void __launch_bounds__(256, 4) k_oz_split_cols(OzOperand B, int N, in
       if (i >= s) continue;
       int8_t* d0 = r0 + (size_t)i * slice_stride;
       int8_t* d1 = r1 + (size_t)i * slice_stride;
+      // the slices of -Im are the negated slices of Im (truncation is odd):
+      // a byte-wise negation of the packed digits
+      const uint32_t wnim = __vneg4(wim[i]);
       if (vec && k + 3 < Kc) {
         *reinterpret_cast<uint32_t*>(d0 + k) = wre[i];
-        *reinterpret_cast<uint32_t*>(d0 + Kc + k) = wnim[i];
+        *reinterpret_cast<uint32_t*>(d0 + Kc + k) = wnim;
         *reinterpret_cast<uint32_t*>(d1 + k) = wim[i];
         *reinterpret_cast<uint32_t*>(d1 + Kc + k) = wre[i];
       } else {
         for (int c = 0; c < 4 && k + c < Kc; c++) {
           d0[k + c] = (int8_t)(wre[i] >> (8 * c));
-          d0[Kc + k + c] = (int8_t)(wnim[i] >> (8 * c));
+          d0[Kc + k + c] = (int8_t)(wnim >> (8 * c));
           d1[k + c] = (int8_t)(wim[i] >> (8 * c));
           d1[Kc + k + c] = (int8_t)(wre[i] >> (8 * c));
         }
