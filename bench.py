@@ -763,6 +763,7 @@ def run_zgemm_split(args):
     zgemm_ms = time_cublas()
     flops = 8.0 * M * N * K * batch
     out = {}
+    lib.tups_set_split_cta_pairs(1 if args.cta_pairs else 0)
     for nt in args.n_tile:
         if lib.tups_set_split_tile(nt):
             raise RuntimeError(f"tups_set_split_tile({nt}) refused")
@@ -791,7 +792,8 @@ def run_zgemm_split(args):
     lib.tups_set_split_tile(0)
     zgemm_ms = min(zgemm_ms, time_cublas())
     line = {"metric": "split ZGEMM effective TFLOP/s", "unit": "TFLOP/s", "workload": ZGEMM_WORKLOAD,
-            "config": {"Nz": Nz, "batch": batch, "M": M, "N": N, "K": K}, "steps": reps,
+            "config": {"Nz": Nz, "batch": batch, "M": M, "N": N, "K": K, "cta_pairs": bool(args.cta_pairs)},
+            "steps": reps,
             "cublas_zgemm_ms": zgemm_ms, "cublas_zgemm_tflops": flops / zgemm_ms / 1e9, "slices": out}
     print(json.dumps(line), flush=True)
 
@@ -808,6 +810,8 @@ def main():
     ap.add_argument("--slices", type=int, nargs="+", default=[2, 3, 4, 5, 6, 7, 8], help="zgemm_split: slice counts")
     ap.add_argument("--n-tile", type=int, nargs="+", default=[0],
                     help="zgemm_split: column tiles of the split GEMM to compare (0 = automatic)")
+    ap.add_argument("--cta-pairs", action="store_true",
+                    help="zgemm_split: run the split GEMM on CTA pairs (M = 256 tiles over two SMs)")
     ap.add_argument("--lu-q", type=int, default=64,
                     help="bse_lu_1024: momenta (x 16 frequencies = instances); fewer for a small profiling case")
     ap.add_argument("--crossing-products", type=int, default=0, choices=[0, 3, 4],

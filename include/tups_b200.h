@@ -268,6 +268,11 @@ int tups_set_split_wait(long long cycles, int stall_test);
  * integer slice sums are exact and the FP64 folding order is fixed).
  * Process-wide; no counterpart in the reference. */
 int tups_set_split_tile(int n_tile);
+/* The split GEMM on CTA pairs: enable = 1 runs row counts >= 256 as
+ * 256 x n_tile tiles over two SMs (tcgen05 cta_group::2, each SM staging
+ * half of the B operand), 0 (default) as 128 x n_tile tiles on one SM each.
+ * Both give the same bits.  Process-wide; no counterpart in the reference. */
+int tups_set_split_cta_pairs(int enable);
 
 /* ---- tile-shape tuner -------------------------------------------------------
  * No counterpart in the reference.  The first FP64 BSE GEMM and the first

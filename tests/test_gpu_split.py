@@ -51,6 +51,25 @@ def test_zgemm_split_matches_the_emulation(gpu_lib, dims, s):
         assert parity.rel(got[b], exact) <= 10.0 ** (1.6 - 2.0 * s) + 1e-14
 
 
+@pytest.mark.parametrize("dims", [(2, 256, 80, 64), (1, 300, 150, 300)], ids=["pair", "pair_ragged"])
+@pytest.mark.parametrize("s", [3, 8])
+def test_zgemm_split_cta_pairs_match_the_emulation(gpu_lib, dims, s):
+    """The CTA-pair form (M = 256 tiles over two SMs) writes the emulation's
+    result like the one-SM form."""
+    batch, M, N, K = dims
+    rng = np.random.default_rng(7 * M + N + K + s)
+    A = (rng.normal(size=(batch, M, K)) + 1j * rng.normal(size=(batch, M, K))) * np.logspace(-2, 2, K)[None, None, :]
+    B = rng.normal(size=(batch, K, N)) + 1j * rng.normal(size=(batch, K, N))
+    gpu_lib.tups_set_split_cta_pairs(1)
+    try:
+        got = _zgemm_split(gpu_lib, A, B, s)
+    finally:
+        gpu_lib.tups_set_split_cta_pairs(0)
+    for b in range(batch):
+        emu = S.ozaki_zgemm(A[b], B[b], s)
+        assert parity.rel(got[b], emu) <= EMU_TOL, (b, parity.rel(got[b], emu))
+
+
 def test_split_bse_against_fp64(gpu_lib):
     from oracle import tups_oracle as O
     from tups_b200 import Solver

@@ -104,6 +104,7 @@ _PROTOS = {
     "tups_set_crossing_products": [C.c_void_p, C.c_int],
     "tups_set_split_wait": [C.c_longlong, C.c_int],
     "tups_set_split_tile": [C.c_int],
+    "tups_set_split_cta_pairs": [C.c_int],
     "tups_bse_lu_split_batched": [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double),
                                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_int,
                                   C.c_void_p, C.c_size_t, C.POINTER(C.c_int), C.POINTER(C.c_double),

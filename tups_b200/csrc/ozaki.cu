@@ -665,12 +665,342 @@ __global__ void __launch_bounds__(OZ_THREADS2, 1)
   }
 }
 
+// ---- the GEMM on CTA pairs (tcgen05 cta_group::2) ------------------------------
+// The same tiles, diagonal schedule and FP64 folding as k_oz_gemm (so the
+// same bits), but a cluster of two CTAs computes a 256 x n_tile tile with
+// one M = 256 MMA per K step: CTA r stages rows 128 r .. 128 r + 127 of the
+// pair's A rows and half of the tile's B columns (n_tile / 2 rows of B'), so
+// each SM's tensor core reads 4 KB + n_tile x 16 B of operands per MMA
+// instead of 4 KB + n_tile x 32 B.  The leader (cluster rank 0) issues the
+// MMAs and owns the stage-full barriers (both CTAs' copies complete there);
+// the MMA completions reach both CTAs' stage-empty and accumulator-full
+// barriers by multicast commits; each CTA's drain warps read their own TMEM
+// rows and arrive on the leader's accumulator-empty barrier.  Only the
+// tensor maps of this GPU's own memory are read, and no copy multicasts.
+constexpr int OZ2_STAGES = 8;  // 8 x (16 KB of A + <= 8 KB of B)
+
+__device__ __forceinline__ uint32_t oz_cluster_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+// the shared::cluster address of `addr` (a shared::cta address) in CTA `rank`
+__device__ __forceinline__ uint32_t oz_mapa(uint32_t addr, uint32_t rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(addr), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ void oz_cluster_sync() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+__device__ __forceinline__ bool mbar_try_cl(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(oz_smem(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait with cluster-scope acquire (barriers that other CTAs signal)
+__device__ __forceinline__ bool mbar_wait_cl(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
+                                             bool honor_abort = true, long long limit = OZ_WAIT_CYCLES) {
+  const long long t0 = clock64();
+  for (uint32_t it = 0;; it++) {
+    if (mbar_try_cl(bar, parity)) return true;
+    if ((it & 255) == 255) {
+      if (honor_abort && *abort_flag) return false;
+      if (clock64() - t0 > limit) {
+        *abort_flag = 1;
+        return false;
+      }
+    }
+  }
+}
+__device__ __forceinline__ void mbar_arrive_remote(uint32_t cluster_addr) {
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr) : "memory");
+}
+__device__ __forceinline__ void tma_load_2d_pair(uint32_t dst, const CUtensorMap* map, int x, int y,
+                                                 uint32_t bar_cluster) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, "
+      "%3}], [%4];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar_cluster)
+      : "memory");
+}
+// MMA completion to the barrier at this offset in the CTAs of `mask`
+__device__ __forceinline__ void tc_commit_pair(uint64_t* bar, uint16_t mask) {
+  asm volatile(
+      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
+          oz_smem(bar)),
+      "h"(mask)
+      : "memory");
+}
+__device__ __forceinline__ void tc_mma_i8_pair(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                               uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::2.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8, %9, %10, %11, %12}, p;\n\t}" ::"r"(
+          d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u), "r"(0u), "r"(0u),
+      "r"(0u), "r"(0u));
+}
+
+// P.m_tiles counts 256-row pair tiles here
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(OZ_THREADS2, 1)
+    k_oz_gemm2(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, OzGemm P) {
+  extern __shared__ uint8_t oz_dyn[];
+  __shared__ uint64_t full_bar[OZ2_STAGES], empty_bar[OZ2_STAGES], accf_bar[OZ_NBUF], acce_bar[OZ_NBUF], done_bar;
+  __shared__ uint64_t never_bar;
+  __shared__ uint32_t tmem_base_sh;
+  __shared__ volatile int abort_sh;
+  __shared__ int issued_sh, consumed_sh;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t crank = oz_cluster_rank();
+  const bool leader = crank == 0;
+  const int Np = 2 * P.N;
+  const int NT = P.n_tile, HB = NT >> 1;  // B' rows staged by each CTA
+  const uint32_t a_bytes = OZ_BM * OZ_BK, b_bytes = (uint32_t)HB * OZ_BK;
+  const uint32_t dyn = (oz_smem(oz_dyn) + 1023u) & ~1023u;
+  auto sA = [&](int st) { return dyn + (uint32_t)st * (a_bytes + b_bytes); };
+  auto sB = [&](int st) { return dyn + (uint32_t)st * (a_bytes + b_bytes) + a_bytes; };
+  const int per_inst = P.m_tiles * P.n_tiles;
+  const int cid = blockIdx.x >> 1, ncl = gridDim.x >> 1;
+
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < OZ2_STAGES; i++) {
+      mbar_init(&full_bar[i], 1);
+      mbar_init(&empty_bar[i], 1);
+    }
+    for (int i = 0; i < OZ_NBUF; i++) {
+      mbar_init(&accf_bar[i], 1);
+      mbar_init(&acce_bar[i], 2 * OZ_DRAIN_WARPS * 32);
+    }
+    mbar_init(&done_bar, 1);
+    mbar_init(&never_bar, 1);
+    abort_sh = 0;
+    issued_sh = 0;
+    consumed_sh = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == OZ_DRAIN_WARPS) {
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(oz_smem(&tmem_base_sh)),
+                 "r"(512u));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  // both CTAs' barriers exist before either CTA signals the other's
+  oz_cluster_sync();
+  tc_fence_after();
+  const uint32_t tmem = tmem_base_sh;
+
+  if (warp == OZ_DRAIN_WARPS + 1) {
+    // ---- TMA producer (both CTAs): own rows of A, own half of B' ----
+    if (lane == 0) {
+      int stage = 0;
+      uint32_t phase = 0;
+      int issued = 0;
+      bool ok = true;
+      for (int t = cid; t < P.tiles && ok; t += ncl) {
+        const int inst = t / per_inst, rem = t % per_inst;
+        const int m0 = (rem % P.m_tiles) * (2 * OZ_BM) + (int)crank * OZ_BM;
+        const int n0 = (rem / P.m_tiles) * NT + (int)crank * HB;
+        for (int d = 0; d < P.s && ok; d++)
+          for (int i = 0; i <= d && ok; i++) {
+            const int ya = (inst * P.s + i) * P.M + m0;
+            const int yb = (inst * P.s + (d - i)) * Np + n0;
+            for (int kc = 0; kc < P.kchunks; kc++) {
+              if (!mbar_wait_cl(&empty_bar[stage], phase ^ 1u, &abort_sh, true, P.wait_cycles)) {
+                ok = false;
+                break;
+              }
+              // the leader's stage-full barrier counts both CTAs' bytes
+              if (leader) mbar_expect_tx(&full_bar[stage], 2 * (a_bytes + b_bytes));
+              const uint32_t fb = oz_mapa(oz_smem(&full_bar[stage]), 0);
+              tma_load_2d_pair(sA(stage), &tmA, kc * OZ_BK, ya, fb);
+              tma_load_2d_pair(sB(stage), &tmB, kc * OZ_BK, yb, fb);
+              issued++;
+              if (++stage == OZ2_STAGES) {
+                stage = 0;
+                phase ^= 1u;
+              }
+            }
+          }
+      }
+      issued_sh = issued;
+    }
+  } else if (warp == OZ_DRAIN_WARPS) {
+    // ---- MMA issuer: the leader only ----
+    if (lane == 0 && leader) {
+      const uint32_t idesc = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NT >> 3) << 17) |
+                             ((uint32_t)((2 * OZ_BM) >> 4) << 24);
+      int stage = 0;
+      uint32_t phase = 0;
+      int consumed = 0;
+      int nacc = 0;
+      bool ok = true;
+      if (P.stall_test) ok = mbar_wait(&never_bar, 0, &abort_sh, true, P.wait_cycles);
+      for (int t = cid; t < P.tiles && ok; t += ncl)
+        for (int d = 0; d < P.s && ok; d++, nacc++) {
+          const int buf = nacc % OZ_NBUF;
+          if (nacc >= OZ_NBUF &&
+              !mbar_wait_cl(&acce_bar[buf], (uint32_t)((nacc - OZ_NBUF) / OZ_NBUF) & 1u, &abort_sh, true,
+                            P.wait_cycles)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t dtm = tmem + (uint32_t)(buf * OZ_MAX_NT);
+          uint32_t accum = 0;
+          for (int i = 0; i <= d && ok; i++)
+            for (int kc = 0; kc < P.kchunks; kc++) {
+              if (!mbar_wait_cl(&full_bar[stage], phase, &abort_sh, true, P.wait_cycles)) {
+                ok = false;
+                break;
+              }
+              consumed++;
+              tc_fence_after();
+              const uint64_t da = oz_desc(sA(stage)), db = oz_desc(sB(stage));
+#pragma unroll
+              for (int kk = 0; kk < OZ_BK / 32; kk++) {
+                tc_mma_i8_pair(dtm, da + 2 * kk, db + 2 * kk, idesc, accum);
+                accum = 1;
+              }
+              tc_commit_pair(&empty_bar[stage], 0x3);
+              if (++stage == OZ2_STAGES) {
+                stage = 0;
+                phase ^= 1u;
+              }
+            }
+          if (ok) tc_commit_pair(&accf_bar[buf], 0x3);
+        }
+      consumed_sh = consumed;
+      tc_commit_pair(&done_bar, 0x1);
+      mbar_wait_cl(&done_bar, 0, &abort_sh, false);
+    }
+  } else {
+    // ---- drain (both CTAs): own TMEM lanes = own 128 rows of the pair tile ----
+    const int quarter = warp & 3, h = warp >> 2;
+    const int half = NT >> 1;
+    const int row = quarter * 32 + lane;
+    const uint32_t acce_leader0 = oz_mapa(oz_smem(&acce_bar[0]), 0);
+    double acc[OZ_HALF];
+    int nacc = 0;
+    bool ok = true;
+    for (int t = cid; t < P.tiles && ok; t += ncl) {
+      const int inst = t / per_inst, rem = t % per_inst;
+      const int m0 = (rem % P.m_tiles) * (2 * OZ_BM) + (int)crank * OZ_BM;
+      const int n0 = (rem / P.m_tiles) * NT;
+      const int m = m0 + row;
+      const bool mok = m < P.M;
+#pragma unroll
+      for (int c = 0; c < OZ_HALF; c++) acc[c] = 0.0;
+      for (int d = 0; d < P.s; d++, nacc++) {
+        const int buf = nacc % OZ_NBUF;
+        if (!mbar_wait_cl(&accf_bar[buf], (uint32_t)(nacc / OZ_NBUF) & 1u, &abort_sh, true, P.wait_cycles)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const double w = ldexp(1.0, -OZ_SLICE_BITS * (d + 2));
+        const uint32_t tb = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(buf * OZ_MAX_NT + h * half);
+#pragma unroll
+        for (int c = 0; c < OZ_HALF; c += 8) {
+          if (c < half) {
+            int32_t v[8];
+            tc_ld8(tb + (uint32_t)c, v);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int e = 0; e < 8; e++) acc[c + e] = fma((double)v[e], w, acc[c + e]);
+          }
+        }
+        tc_fence_before();
+        mbar_arrive_remote(acce_leader0 + (uint32_t)(buf * sizeof(uint64_t)));
+      }
+      if (!ok) break;
+      if (!mok) continue;
+      const double rs = P.rscale[(size_t)inst * P.M + m];
+      cplx* Cq = nullptr;
+      const cplx* Fq = nullptr;
+      cplx* Gq = nullptr;
+      int r = 0;
+      if (P.epi == OZ_EPI_BSE) {
+        const int q = P.q_begin + inst / 4;
+        r = inst % 4;
+        const cplx* Fr = r == 0 ? P.F[0] : r == 1 ? P.F[1] : r == 2 ? P.F[2] : P.F[3];
+        cplx* Gr = r == 0 ? P.G[0] : r == 1 ? P.G[1] : r == 2 ? P.G[2] : P.G[3];
+        Fq = Fr + (size_t)P.M * P.M * q;
+        Gq = Gr + (size_t)P.M * P.M * q;
+      } else if (P.epi == OZ_EPI_SUB) {
+        Cq = P.C + (size_t)inst * P.c_stride;
+      } else {
+        Cq = P.C + (size_t)inst * P.M * P.N;
+      }
+      const double sr = r == 0 ? P.scale[0] : r == 1 ? P.scale[1] : r == 2 ? P.scale[2] : P.scale[3];
+#pragma unroll
+      for (int c = 0; c < OZ_HALF; c += 2) {
+        const int np = n0 + h * half + c;
+        if (c < half && np < Np) {
+          const int jc = np >> 1;
+          const double sc = rs * P.cscale[(size_t)inst * P.N + jc];
+          const double cre = acc[c] * sc, cim = acc[c + 1] * sc;
+          if (P.epi == OZ_EPI_SUB) {
+            const size_t ix = m + (size_t)P.ldc * jc;
+            const cplx c0 = Cq[ix];
+            Cq[ix] = cmk(c0.x - cre, c0.y - cim);
+            continue;
+          }
+          const size_t idx = m + (size_t)P.M * jc;
+          if (P.epi == OZ_EPI_ZGEMM) {
+            Cq[idx] = cmk(cre, cim);
+          } else {
+            const cplx f = Fq[idx], g = Gq[idx];
+            Gq[idx] = cmk(__dadd_rn(__dmul_rn(sr, cre), __dmul_rn(P.omf, __dsub_rn(f.x, g.x))),
+                          __dadd_rn(__dmul_rn(sr, cim), __dmul_rn(P.omf, __dsub_rn(f.y, g.y))));
+          }
+        }
+      }
+    }
+  }
+
+  __syncthreads();
+  if (threadIdx.x == 0 && abort_sh) {
+    *P.status = P.status_code;
+    if (leader) {
+      // wait for the stages whose copies were issued but never consumed
+      int stage = consumed_sh % OZ2_STAGES;
+      uint32_t phase = (uint32_t)(consumed_sh / OZ2_STAGES) & 1u;
+      for (int k = consumed_sh; k < issued_sh; k++) {
+        mbar_wait_cl(&full_bar[stage], phase, &abort_sh, false);
+        if (++stage == OZ2_STAGES) {
+          stage = 0;
+          phase ^= 1u;
+        }
+      }
+    }
+  }
+  __syncthreads();
+  // neither CTA frees its shared or tensor memory while the other may still use it
+  oz_cluster_sync();
+  if (warp == OZ_DRAIN_WARPS) {
+    __syncwarp();
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512u));
+  }
+}
+
 // ---- host side ----------------------------------------------------------------------
 // the work loop's wait limit (0: OZ_WAIT_CYCLES) and a pending stall test,
 // set by tups_set_split_wait; the stall test applies to the next launch only
 static std::atomic<long long> g_oz_wait_cycles{0};
 static std::atomic<int> g_oz_stall_test{0};
 static std::atomic<int> g_oz_n_tile{0};  // 0: oz_n_tile
+static std::atomic<int> g_oz_pairs{0};   // 1: k_oz_gemm2 (CTA pairs) for M >= 256
 
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
@@ -784,11 +1114,14 @@ int oz_run(OzRun& R, cudaStream_t stream, long long* launches) {
   P.N = N;
   P.s = s;
   P.kchunks = Kpad / OZ_BK;
+  const bool pairs = g_oz_pairs.load() != 0 && M >= 2 * OZ_BM;
   {
     const int nt = g_oz_n_tile.load();
     P.n_tile = nt > 0 ? nt : oz_n_tile(N);
+    // CTA pairs: each CTA stages n_tile / 2 rows of B', a multiple of 16
+    if (pairs) P.n_tile = std::min(OZ_MAX_NT, (P.n_tile + 31) / 32 * 32);
   }
-  P.m_tiles = (M + OZ_BM - 1) / OZ_BM;
+  P.m_tiles = pairs ? (M + 2 * OZ_BM - 1) / (2 * OZ_BM) : (M + OZ_BM - 1) / OZ_BM;
   P.n_tiles = (2 * N + P.n_tile - 1) / P.n_tile;
   if ((long long)batch * P.m_tiles * P.n_tiles >= (1LL << 31)) return TUPS_ERR_BADDIM;
   P.tiles = batch * P.m_tiles * P.n_tiles;
@@ -815,14 +1148,25 @@ int oz_run(OzRun& R, cudaStream_t stream, long long* launches) {
   CUtensorMap ta, tb;
   if (!make_map(&ta, R.a_slices, (long long)batch * s * M, Kpad, OZ_BM))
     return oz_fail("tensor map of the A slices", cudaSuccess);
-  if (!make_map(&tb, R.b_slices, (long long)batch * s * 2 * N, Kpad, P.n_tile))
+  if (!make_map(&tb, R.b_slices, (long long)batch * s * 2 * N, Kpad, pairs ? P.n_tile / 2 : P.n_tile))
     return oz_fail("tensor map of the B slices", cudaSuccess);
-  const size_t smem = oz_smem_bytes(P.n_tile);
-  cudaError_t e = cudaFuncSetAttribute(k_oz_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return oz_fail("k_oz_gemm shared memory attribute", e);
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaError_t e;
+  if (pairs) {
+    const size_t smem = (size_t)OZ2_STAGES * (OZ_BM * OZ_BK + (size_t)(P.n_tile / 2) * OZ_BK) + 1024;
+    e = cudaFuncSetAttribute(k_oz_gemm2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return oz_fail("k_oz_gemm2 shared memory attribute", e);
+    const int grid = 2 * std::max(1, std::min(P.tiles, sms / 2));
+    k_oz_gemm2<<<grid, OZ_THREADS2, smem, stream>>>(ta, tb, P);
+    if (launches) (*launches)++;
+    e = cudaGetLastError();
+    return e == cudaSuccess ? TUPS_OK : oz_fail("k_oz_gemm2 launch", e);
+  }
+  const size_t smem = oz_smem_bytes(P.n_tile);
+  e = cudaFuncSetAttribute(k_oz_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return oz_fail("k_oz_gemm shared memory attribute", e);
   const int grid = std::max(1, std::min(P.tiles, sms));
   k_oz_gemm<<<grid, OZ_THREADS2, smem, stream>>>(ta, tb, P);
   if (launches) (*launches)++;
@@ -894,5 +1238,14 @@ extern "C" int tups_set_split_wait(long long cycles, int stall_test) {
 extern "C" int tups_set_split_tile(int n_tile) {
   if (n_tile < 0 || n_tile > tups::OZ_MAX_NT || n_tile % 16) return TUPS_ERR_BADARG;
   tups::g_oz_n_tile.store(n_tile);
+  return TUPS_OK;
+}
+
+// The split GEMM on CTA pairs (tcgen05 cta_group::2, M = 256 over two SMs)
+// for row counts >= 256: 1 enables, 0 restores one CTA per 128-row tile.
+// Both forms give the same bits.  Process-wide; no counterpart in the
+// reference.
+extern "C" int tups_set_split_cta_pairs(int enable) {
+  tups::g_oz_pairs.store(enable ? 1 : 0);
   return TUPS_OK;
 }
