@@ -27,17 +27,25 @@ struct BsePtrs {
 // chi Gamma: it loads the Nl entries of Gamma that the line needs once and
 // forms all Nl outputs from registers (sums in l ascending order).  LMAX >= Nl
 // sizes the register array (instantiated for the shell counts 1, 5, 9, 13).
+// The grid strides over (instance, line) pairs, a few CTAs per SM, so the
+// short per-line work is not paced by CTA launches.
 template <int LMAX>
-__global__ void k_bse_prep(BsePtrs P, const cplx* __restrict__ chi_ph, const cplx* __restrict__ chi_pp,
-                           cplx* __restrict__ A, cplx* __restrict__ B, int q_begin, int Nz, int Nf, int Nl) {
-  const int inst = blockIdx.y;
-  const int q = q_begin + inst / 4, r = inst % 4;
-  const cplx* chi = (r < 2 ? chi_ph : chi_pp) + (size_t)Nl * Nl * Nf * q;
-  const cplx* Gm = P.G[r] + (size_t)Nz * Nz * q;
-  cplx* Ai = A + (size_t)Nz * Nz * inst;
-  cplx* Bi = B + (size_t)Nz * Nz * inst;
+__global__ void __launch_bounds__(256) k_bse_prep(BsePtrs P, const cplx* __restrict__ chi_ph,
+                                                  const cplx* __restrict__ chi_pp, cplx* __restrict__ A,
+                                                  cplx* __restrict__ B, int q_begin, int n_inst, int Nz, int Nf,
+                                                  int Nl) {
   const size_t lines = (size_t)Nz * Nf;
-  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < 2 * lines; t += (size_t)gridDim.x * blockDim.x) {
+  const size_t total = 2 * lines * (size_t)n_inst;
+  for (size_t x = (size_t)blockIdx.x * blockDim.x + threadIdx.x; x < total; x += (size_t)gridDim.x * blockDim.x) {
+    const int inst = (int)(x / (2 * lines));
+    const size_t t = x - (size_t)inst * 2 * lines;
+    const int q = q_begin + inst / 4, r = inst % 4;
+    const cplx* chi = (r < 2 ? chi_ph : chi_pp) + (size_t)Nl * Nl * Nf * q;
+    // constant indices keep the parameter struct out of local memory
+    const cplx* Gr = r == 0 ? P.G[0] : r == 1 ? P.G[1] : r == 2 ? P.G[2] : P.G[3];
+    const cplx* Gm = Gr + (size_t)Nz * Nz * q;
+    cplx* Ai = A + (size_t)Nz * Nz * inst;
+    cplx* Bi = B + (size_t)Nz * Nz * inst;
     cplx g[LMAX];
     if (t < lines) {
       // A[row, (l2, nu)] = sum_l1 Gamma[row, (l1, nu)] chi[l1, l2, nu]
@@ -449,13 +457,16 @@ int launch_bse_chunk(tups_ctx* ctx, int q_begin, int q_count) {
   }
   const int slices = ctx->cur_slices;
   if (d.Nl > 16) return set_error(ctx, TUPS_ERR_BADDIM, "Nl > 16 not supported by k_bse_prep");
-  const size_t lines2 = (size_t)2 * d.Nz * d.Nf;
-  dim3 pgrid((unsigned)std::min<size_t>(cdiv(lines2, 256), 4096), 4 * q_count);
+  const size_t lines2 = (size_t)2 * d.Nz * d.Nf * 4 * q_count;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const unsigned pgrid = (unsigned)std::min<size_t>(cdiv(lines2, 256), (size_t)sms * 8);
   phase_begin(ctx, TUPS_PHASE_BSE_PREP);
   auto prep = d.Nl <= 1 ? k_bse_prep<1> : d.Nl <= 5 ? k_bse_prep<5> : d.Nl <= 9 ? k_bse_prep<9>
              : d.Nl <= 13 ? k_bse_prep<13> : k_bse_prep<16>;
-  prep<<<pgrid, 256, 0, ctx->stream>>>(P, ctx->s.chi_ph, ctx->s.chi_pp, ctx->s.bse_A, ctx->s.bse_B, q_begin, d.Nz,
-                                       d.Nf, d.Nl);
+  prep<<<pgrid, 256, 0, ctx->stream>>>(P, ctx->s.chi_ph, ctx->s.chi_pp, ctx->s.bse_A, ctx->s.bse_B, q_begin,
+                                       4 * q_count, d.Nz, d.Nf, d.Nl);
   int rc = after_launch(ctx, "k_bse_prep");
   phase_end(ctx, TUPS_PHASE_BSE_PREP);
   if (rc) return rc;
