@@ -607,9 +607,18 @@ extern "C" int tups_get_sde_aux(tups_ctx* ctx, double* cph, double* cpp, double*
   const size_t na = (size_t)d.Nl * d.nbox * d.Nb * sizeof(cplx), nz = (size_t)d.Nz * d.Nb * sizeof(cplx);
   if (cph) TRY(copy_d2h(ctx, cph, ctx->s.chi_aux_ph, na));
   if (cpp) TRY(copy_d2h(ctx, cpp, ctx->s.chi_aux_pp, na));
-  if (lchi) TRY(copy_d2h(ctx, lchi, ctx->s.LChi, nz));
-  if (phchi) TRY(copy_d2h(ctx, phchi, ctx->s.PhChi, nz));
-  if (ppchi) TRY(copy_d2h(ctx, ppchi, ctx->s.PPChi, nz));
+  // the device keeps these slot-fastest (Nb, Nz); the caller gets (Nz, Nb)
+  std::vector<cplx> tmp;
+  const cplx* src[3] = {ctx->s.LChi, ctx->s.PhChi, ctx->s.PPChi};
+  double* dst[3] = {lchi, phchi, ppchi};
+  for (int a = 0; a < 3; a++) {
+    if (!dst[a]) continue;
+    tmp.resize((size_t)d.Nz * d.Nb);
+    TRY(copy_d2h(ctx, tmp.data(), src[a], nz));
+    cplx* out = reinterpret_cast<cplx*>(dst[a]);
+    for (size_t q = 0; q < (size_t)d.Nb; q++)
+      for (size_t i = 0; i < (size_t)d.Nz; i++) out[i + d.Nz * q] = tmp[q + d.Nb * i];
+  }
   return TUPS_OK;
 }
 extern "C" int tups_synchronize(tups_ctx* ctx) {

@@ -22,7 +22,9 @@ __device__ __forceinline__ int pick_range(int j, int Nf, int fr) {
   return Nf;
 }
 
-// LChi, PhChi, PPChi (Nz, Nb): 32 rows x 8 column groups per CTA, one slot q
+// LChi, PhChi, PPChi stored slot-fastest, (Nb, Nz): element (i, q) at
+// q + Nb i, so that k_sde_sigma's lanes (consecutive slots) read
+// consecutive addresses.  32 rows x 8 column groups per CTA, one slot q
 __global__ void k_sde_chis(SdePtrs P, const cplx* __restrict__ cph, const cplx* __restrict__ cpp,
                            const int* __restrict__ ibz, cplx* __restrict__ LChi, cplx* __restrict__ PhChi,
                            cplx* __restrict__ PPChi, int Nz, int Nf, int Nl, int fr, int use_U2, double U,
@@ -79,7 +81,7 @@ __global__ void k_sde_chis(SdePtrs P, const cplx* __restrict__ cph, const cplx* 
     ph = cadd(ph, red_ph[y][threadIdx.x]);
     pp = cadd(pp, red_pp[y][threadIdx.x]);
   }
-  const size_t o = (size_t)i + (size_t)Nz * q;
+  const size_t o = (size_t)q + (size_t)gridDim.y * i;  // gridDim.y = Nb
   LChi[o] = lc;
   PhChi[o] = ph;
   PPChi[o] = pp;
@@ -114,9 +116,10 @@ __global__ void __launch_bounds__(256) k_sde_sigma(const cplx* __restrict__ Gkw,
     // local slot q of this context is global slot slot0 + q
     const int w = ibz[3 * (slot0 + q) + 2];
     const int Qi = (slot0 + q) / nh;
-    const cplx* Lq = LChi + (size_t)Nz * q;
-    const cplx* Pq = PhChi + (size_t)Nz * q;
-    const cplx* Qq = PPChi + (size_t)Nz * q;
+    // row i of slot q at q + Nb i
+    const cplx* Lq = LChi + q;
+    const cplx* Pq = PhChi + q;
+    const cplx* Qq = PPChi + q;
     cplx acc = cmk(0.0, 0.0);
     for (int s = 0; s < NS; s++) {
       if (!symlist[NS * Qi + s]) continue;
@@ -129,12 +132,12 @@ __global__ void __launch_bounds__(256) k_sde_sigma(const cplx* __restrict__ Gkw,
           get_green(Gkw, SigmaH, Ek, (Nx - qmkx) % Nx, (Ny - qmky) % Ny, -qmkw + Nf + 1, Nx, Ny, Nf, beta, mu);
       for (int l3 = 0; l3 < Nl; l3++) {
         const double ffi = FFinv[s + NS * (kx + Nx * (ky + Ny * l3))];
-        const int i3 = l3 * Nf + k0 - 1;
+        const size_t i3 = (size_t)Nb * (l3 * Nf + k0 - 1);
         acc = cadd(acc, cscale(cmul(gkq, Lq[i3]), ffi));
         acc = cadd(acc, cscale(cmul(gkq, Pq[i3]), ffi));
         acc = cadd(acc, cscale(cmul(gqmk, Qq[i3]), ffi));
         if (w == 1) continue;
-        const int i3m = l3 * Nf + Nf - k0;
+        const size_t i3m = (size_t)Nb * (l3 * Nf + Nf - k0);
         const double fs = ffi * (double)signs[l3];
         acc = cadd(acc, cscale(cmul(gkmq, cconj(Lq[i3m])), fs));
         acc = cadd(acc, cscale(cmul(gkmq, cconj(Pq[i3m])), fs));

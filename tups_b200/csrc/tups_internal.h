@@ -57,7 +57,7 @@ struct DeviceState {
   cplx* M[4] = {};            // (Nl^4, NIBZ, NR): 0 phbar_to_ph 1 pp_to_ph 2 ph_to_pp 3 phbar_to_pp
   cplx* chi_aux_ph = nullptr; // (Nl*nbox, Nb)
   cplx* chi_aux_pp = nullptr;
-  cplx* LChi = nullptr;       // (Nz, Nb)
+  cplx* LChi = nullptr;       // (Nb, Nz): slot fastest
   cplx* PhChi = nullptr;
   cplx* PPChi = nullptr;
   cplx* SigmaV = nullptr;     // (NIBZ*Nf)
