@@ -295,6 +295,13 @@ int tups_set_crossing_products(tups_ctx* ctx, int products);
  * most len bytes (NUL-terminated) and returns the length the whole table
  * needs, NUL included; buf may be NULL with len 0 to ask for it. */
 int tups_get_tuning(char* buf, size_t len);
+/* Fix the candidate named `name` for every tuner key that starts with
+ * key_prefix (e.g. "k_pae_mma(3M) Nl=5"), in this process, ahead of the
+ * tuner and its cached choices; a key whose candidates do not include the
+ * name keeps the tuner's choice.  name = NULL drops that prefix's entry;
+ * key_prefix = NULL drops all.  Every candidate writes the same bits, so
+ * this only selects a launch shape (for tests and profiling). */
+int tups_set_tuning(const char* key_prefix, const char* name);
 
 /* ---- multilayer perceptron of the learned warm start ------------------------
  * No counterpart in the reference.  FP32 network n_in -> n_hidden (x n_layers,

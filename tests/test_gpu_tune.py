@@ -46,3 +46,39 @@ def test_tuned_tiles_equal_default_tiles(gpu_lib, case):
         # the pick is the fastest candidate, so never slower than the default (index 0)
         assert float(ms[choice]) <= float(ms[names[0]])
         assert float(ms[choice]) == min(float(v) for v in ms.values())
+
+
+@pytest.mark.parametrize("case,names", [
+    (dict(Nx=4, Nf=10, neighbours=2), ["g3_flat_bn32_tn2", "g3_flat_bn64_tn4", "g3_flat_bn48_tn3",
+                                       "g3_flat_bn32_tn2_s3", "g3_flat_bn48_tn3_s3", "g3p_flat_bn32_tn2",
+                                       "g3p_flat_bn64_tn4"]),
+    (dict(Nx=8, Nf=6, neighbours=3), ["g3_flat_bn64_tn4", "g3_flat_bn48_tn3", "g3_flat_bn32_tn2",
+                                      "g3_flat_bn48_tn3_s3", "g3_flat_bn32_tn2_s3", "g3p_flat_bn64_tn4",
+                                      "g3p_flat_bn48_tn3"]),
+], ids=["nl5", "nl9"])
+def test_every_crossing_candidate_writes_the_same_bits(gpu_lib, case, names):
+    """Each three-product crossing candidate, fixed by name, against the
+    first: the same F after two full iterations and a third crossing."""
+    from tups_b200 import Params, Solver
+    from tups_b200.parquet import set_tuning
+    p = Params(beta=3.0, U=2.0, nParticle=0.95, f_damping=0.5, ite_max=10, **case)
+    ref = None
+    try:
+        for name in names:
+            set_tuning("k_pae_mma(3M) ", name)
+            sol = Solver(p)
+            for ite in range(2):
+                sol.iteration(ite)
+            sol.calc_Gkw_Grt(2, False)
+            sol.BSE(2)
+            sol.calc_PhiR(2)
+            sol.calculate_PAE()
+            F = [sol.F(r) for r in "dmst"]
+            sol.close()
+            if ref is None:
+                ref = F
+                continue
+            for r in range(4):
+                assert np.array_equal(F[r], ref[r]), (name, r)
+    finally:
+        set_tuning(None, None)

@@ -110,6 +110,7 @@ _PROTOS = {
                                   C.c_void_p, C.c_size_t, C.POINTER(C.c_int), C.POINTER(C.c_double),
                                   C.POINTER(C.c_int), C.c_void_p],
     "tups_get_tuning": [C.c_char_p, C.c_size_t],
+    "tups_set_tuning": [C.c_char_p, C.c_char_p],
     "tups_get_PhiR": [C.c_void_p, C.c_int, C.c_void_p],
     "tups_get_M": [C.c_void_p, C.c_int, C.c_void_p],
     "tups_get_expSqR": [C.c_void_p, C.c_void_p],

@@ -27,25 +27,23 @@ struct BsePtrs {
 // chi Gamma: it loads the Nl entries of Gamma that the line needs once and
 // forms all Nl outputs from registers (sums in l ascending order).  LMAX >= Nl
 // sizes the register array (instantiated for the shell counts 1, 5, 9, 13).
-// The grid strides over (instance, line) pairs, a few CTAs per SM, so the
-// short per-line work is not paced by CTA launches.
+// One row of CTAs per instance (blockIdx.y); every thread takes one line
+// (a grid-stride loop over all instances at a few CTAs per SM was slower at
+// 9 form factors: one line's loads in flight per thread).
 template <int LMAX>
 __global__ void __launch_bounds__(256) k_bse_prep(BsePtrs P, const cplx* __restrict__ chi_ph,
                                                   const cplx* __restrict__ chi_pp, cplx* __restrict__ A,
-                                                  cplx* __restrict__ B, int q_begin, int n_inst, int Nz, int Nf,
-                                                  int Nl) {
+                                                  cplx* __restrict__ B, int q_begin, int Nz, int Nf, int Nl) {
   const size_t lines = (size_t)Nz * Nf;
-  const size_t total = 2 * lines * (size_t)n_inst;
-  for (size_t x = (size_t)blockIdx.x * blockDim.x + threadIdx.x; x < total; x += (size_t)gridDim.x * blockDim.x) {
-    const int inst = (int)(x / (2 * lines));
-    const size_t t = x - (size_t)inst * 2 * lines;
-    const int q = q_begin + inst / 4, r = inst % 4;
-    const cplx* chi = (r < 2 ? chi_ph : chi_pp) + (size_t)Nl * Nl * Nf * q;
-    // constant indices keep the parameter struct out of local memory
-    const cplx* Gr = r == 0 ? P.G[0] : r == 1 ? P.G[1] : r == 2 ? P.G[2] : P.G[3];
-    const cplx* Gm = Gr + (size_t)Nz * Nz * q;
-    cplx* Ai = A + (size_t)Nz * Nz * inst;
-    cplx* Bi = B + (size_t)Nz * Nz * inst;
+  const int inst = blockIdx.y;
+  const int q = q_begin + inst / 4, r = inst % 4;
+  const cplx* chi = (r < 2 ? chi_ph : chi_pp) + (size_t)Nl * Nl * Nf * q;
+  // constant indices keep the parameter struct out of local memory
+  const cplx* Gr = r == 0 ? P.G[0] : r == 1 ? P.G[1] : r == 2 ? P.G[2] : P.G[3];
+  const cplx* Gm = Gr + (size_t)Nz * Nz * q;
+  cplx* Ai = A + (size_t)Nz * Nz * inst;
+  cplx* Bi = B + (size_t)Nz * Nz * inst;
+  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < 2 * lines; t += (size_t)gridDim.x * blockDim.x) {
     cplx g[LMAX];
     if (t < lines) {
       // A[row, (l2, nu)] = sum_l1 Gamma[row, (l1, nu)] chi[l1, l2, nu]
@@ -319,6 +317,13 @@ static int bse_choice(tups_ctx* ctx, const BsePtrs& P, int q_begin, int q_count,
   const int Nz = ctx->d.Nz;
   const std::string key = "k_bse_gemm Nz=" + std::to_string(Nz);
   *choice = 0;
+  std::vector<std::string> names;
+  for (int c = 0; c < kNumBseCands; c++) names.push_back(kBseCands[c].name);
+  const int forced = tune_forced(key, names);
+  if (forced >= 0) {
+    *choice = forced;
+    return TUPS_OK;
+  }
   if (!ctx->autotune || tune_get(key, choice)) return TUPS_OK;
   if (q_begin != 0 || !tune_allowed(ctx)) return TUPS_OK;
   // enough instances for several waves of the smallest tiles
@@ -331,8 +336,6 @@ static int bse_choice(tups_ctx* ctx, const BsePtrs& P, int q_begin, int q_count,
   rc = cuda_check(ctx, cudaMemsetAsync(scratch, 0, 4 * (size_t)qt * n2 * sizeof(cplx), ctx->stream), "tuner scratch");
   BsePtrs T = P;
   for (int r = 0; r < 4; r++) T.G[r] = scratch + (size_t)r * qt * n2;
-  std::vector<std::string> names;
-  for (int c = 0; c < kNumBseCands; c++) names.push_back(kBseCands[c].name);
   if (!rc)
     rc = tune_pick(ctx, key, kNumBseCands, names, [&](int c) { return kBseCands[c].run(ctx, T, 0, qt); }, 2,
                    choice);
@@ -457,16 +460,14 @@ int launch_bse_chunk(tups_ctx* ctx, int q_begin, int q_count) {
   }
   const int slices = ctx->cur_slices;
   if (d.Nl > 16) return set_error(ctx, TUPS_ERR_BADDIM, "Nl > 16 not supported by k_bse_prep");
-  const size_t lines2 = (size_t)2 * d.Nz * d.Nf * 4 * q_count;
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const unsigned pgrid = (unsigned)std::min<size_t>(cdiv(lines2, 256), (size_t)sms * 8);
+  if (4 * q_count > 65535) return set_error(ctx, TUPS_ERR_BADDIM, "k_bse_prep: more than 16383 slots in a chunk");
+  const size_t lines2 = (size_t)2 * d.Nz * d.Nf;
+  const dim3 pgrid((unsigned)std::min<size_t>(cdiv(lines2, 256), 4096), 4 * q_count);
   phase_begin(ctx, TUPS_PHASE_BSE_PREP);
   auto prep = d.Nl <= 1 ? k_bse_prep<1> : d.Nl <= 5 ? k_bse_prep<5> : d.Nl <= 9 ? k_bse_prep<9>
              : d.Nl <= 13 ? k_bse_prep<13> : k_bse_prep<16>;
-  prep<<<pgrid, 256, 0, ctx->stream>>>(P, ctx->s.chi_ph, ctx->s.chi_pp, ctx->s.bse_A, ctx->s.bse_B, q_begin,
-                                       4 * q_count, d.Nz, d.Nf, d.Nl);
+  prep<<<pgrid, 256, 0, ctx->stream>>>(P, ctx->s.chi_ph, ctx->s.chi_pp, ctx->s.bse_A, ctx->s.bse_B, q_begin, d.Nz,
+                                       d.Nf, d.Nl);
   int rc = after_launch(ctx, "k_bse_prep");
   phase_end(ctx, TUPS_PHASE_BSE_PREP);
   if (rc) return rc;

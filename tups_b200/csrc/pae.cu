@@ -161,7 +161,12 @@ __global__ void k_pae_base(PaePtrs P, const int* __restrict__ ibz, int Nz, int N
 // are tabulated once per CTA.
 // G3: three real DMMA products per complex one (P1 = Xr Mr, P2 = Xi Mi,
 // P3 = (Xr + Xi)(Mr + Mi); Re = P1 - P2, Im = P3 - P1 - P2), else four.
-template <int TN, int WN, int RW, int STG, int QN, bool G3 = false>
+// PRE: once a stage has landed, the CTA rewrites its raw (source, k, element)
+// X entries in place as (target, k, element) operands, dispatch factors,
+// conjugation and sign applied (the same operations in the same order as
+// the per-fragment form, so the same bits), behind a second barrier; the
+// MMA warps then load finished fragments.
+template <int TN, int WN, int RW, int STG, int QN, bool G3 = false, bool PRE = false>
 __global__ void __launch_bounds__(32 * RW * WN, RW * WN == 8 ? (TN <= 2 ? PAE_MIN_BLOCKS : 2) : 1)
     k_pae_mma(PaePtrs P, const int4* __restrict__ elems, const int* __restrict__ counts,
               const int* __restrict__ ibz, const int* __restrict__ signs, int Nz, int Nf, int Nl, int NIBZ, int NR,
@@ -301,13 +306,24 @@ __global__ void __launch_bounds__(32 * RW * WN, RW * WN == 8 ? (TN <= 2 ? PAE_MI
 
   // fragment value of element e at k: fa x0 + fb x1, conjugated with sign
   // s(l3) s(l4) for time-reversed elements
-  auto xval = [&](const cplx* cX, int kk, int e, bool trv, double sg, double& re, double& im) {
-    const cplx x0 = cX[kk * LDX + e], x1 = cX[(PAE_BK + kk) * LDX + e];
-    re = fa * x0.x + fb * x1.x;
-    im = fa * x0.y + fb * x1.y;
+  auto combine = [](cplx x0, cplx x1, double a, double b, bool trv, double sg) {
+    double re = __fma_rn(b, x1.x, __dmul_rn(a, x0.x));
+    double im = __fma_rn(b, x1.y, __dmul_rn(a, x0.y));
     if (trv) {
       re = sg * re;
       im = -sg * im;
+    }
+    return cmk(re, im);
+  };
+  auto xval = [&](const cplx* cX, int kk, int e, bool trv, double sg, double& re, double& im) {
+    if (PRE) {  // already combined: target tgt's operand at row tgt
+      const cplx t = cX[(tgt * PAE_BK + kk) * LDX + e];
+      re = t.x;
+      im = t.y;
+    } else {
+      const cplx t = combine(cX[kk * LDX + e], cX[(PAE_BK + kk) * LDX + e], fa, fb, trv, sg);
+      re = t.x;
+      im = t.y;
     }
   };
 
@@ -325,12 +341,25 @@ __global__ void __launch_bounds__(32 * RW * WN, RW * WN == 8 ? (TN <= 2 ? PAE_MI
       if (nk < kt_hi) load_stage(nk % STG, nk);
       else asm volatile("cp.async.commit_group;\n" ::);
     }
-    const cplx* cX = sX + (size_t)(kt % STG) * 2 * PAE_BK * LDX;
+    cplx* cX = sX + (size_t)(kt % STG) * 2 * PAE_BK * LDX;
     const cplx* cB = sB + (size_t)(kt % STG) * BN * PAE_LDB;
+    if (PRE) {
+      // (source 0, source 1) at (k, e) -> (target 0, target 1) at (k, e):
+      // each thread rewrites the entries it read
+      for (int p = tid; p < E * PAE_BK; p += NT) {
+        const int e = p % E, kk = p / E;
+        const cplx x0 = cX[kk * LDX + e], x1 = cX[(PAE_BK + kk) * LDX + e];
+        const bool trv = e_tr[e] != 0;
+        const double sg = ksg[kt * PAE_BK + kk];
+        cX[kk * LDX + e] = combine(x0, x1, fac[0][0], fac[1][0], trv, sg);
+        cX[(PAE_BK + kk) * LDX + e] = combine(x0, x1, fac[0][1], fac[1][1], trv, sg);
+      }
+      __syncthreads();
+    }
 #pragma unroll
     for (int k8 = 0; k8 < PAE_BK; k8 += 8) {
       double are[4], aim[4], anim[4];
-      const double sa = ksg[kt * PAE_BK + k8 + tig], sb = ksg[kt * PAE_BK + k8 + tig + 4];
+      const double sa = PRE ? 1.0 : ksg[kt * PAE_BK + k8 + tig], sb = PRE ? 1.0 : ksg[kt * PAE_BK + k8 + tig + 4];
       xval(cX, k8 + tig, er, tr0, sa, are[0], aim[0]);
       xval(cX, k8 + tig, er + 8, tr1, sa, are[1], aim[1]);
       xval(cX, k8 + tig + 4, er, tr0, sb, are[2], aim[2]);
@@ -390,7 +419,7 @@ __global__ void __launch_bounds__(32 * RW * WN, RW * WN == 8 ? (TN <= 2 ? PAE_MI
     }
 }
 
-template <int TN, int WN, int RW, int STG, int QN = 1, bool G3 = false>
+template <int TN, int WN, int RW, int STG, int QN = 1, bool G3 = false, bool PRE = false>
 static int run_pae(tups_ctx* ctx, const PaePtrs& P, int nchunks, int fam, int max_count) {
   const auto& d = ctx->d;
   constexpr int BN = 8 * TN * WN;
@@ -400,7 +429,7 @@ static int run_pae(tups_ctx* ctx, const PaePtrs& P, int nchunks, int fam, int ma
   const int Kpad = (K + PAE_BK - 1) / PAE_BK * PAE_BK;
   const size_t sm = (size_t)(STG * 2 * PAE_BK * LDX + STG * BN * PAE_LDB) * sizeof(cplx) +
                     (size_t)Kpad * (sizeof(long long) + sizeof(double));
-  auto kern = k_pae_mma<TN, WN, RW, STG, QN, G3>;
+  auto kern = k_pae_mma<TN, WN, RW, STG, QN, G3, PRE>;
   if (sm > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return cuda_check(ctx, e, "k_pae_mma smem attribute");
@@ -502,6 +531,8 @@ static const PaeCand kPaeNl5G3[] = {
     {"g3_flat_bn48_tn3", run_pae<3, 2, 4, 2, 0, true>, 48},
     {"g3_flat_bn32_tn2_s3", run_pae<2, 2, 4, 3, 0, true>, 32},
     {"g3_flat_bn48_tn3_s3", run_pae<3, 2, 4, 3, 0, true>, 48},
+    {"g3p_flat_bn32_tn2", run_pae<2, 2, 4, 2, 0, true, true>, 32},
+    {"g3p_flat_bn64_tn4", run_pae<4, 2, 4, 2, 0, true, true>, 64},
 };
 static const PaeCand kPaeWideG3[] = {
     {"g3_flat_bn64_tn4", run_pae<4, 2, 4, 2, 0, true>, 64},
@@ -509,6 +540,8 @@ static const PaeCand kPaeWideG3[] = {
     {"g3_flat_bn32_tn2", run_pae<2, 2, 4, 2, 0, true>, 32},
     {"g3_flat_bn48_tn3_s3", run_pae<3, 2, 4, 3, 0, true>, 48},
     {"g3_flat_bn32_tn2_s3", run_pae<2, 2, 4, 3, 0, true>, 32},
+    {"g3p_flat_bn64_tn4", run_pae<4, 2, 4, 2, 0, true, true>, 64},
+    {"g3p_flat_bn48_tn3", run_pae<3, 2, 4, 2, 0, true, true>, 48},
 };
 
 static int pae_all(tups_ctx* ctx, const PaePtrs& P, const PaeCand& c) {
@@ -553,9 +586,12 @@ int launch_pae(tups_ctx* ctx) {
                           " NIBZ=" + std::to_string(d.NIBZ) + " NR=" + std::to_string(d.NR) +
                           " Nb=" + std::to_string(d.Nb) + " slot0=" + std::to_string(ctx->slot0);
   int choice = 0;
-  if (ctx->autotune && !tune_get(key, &choice) && tune_allowed(ctx)) {
-    std::vector<std::string> names;
-    for (int c = 0; c < n_cand; c++) names.push_back(cands[c].name);
+  std::vector<std::string> names;
+  for (int c = 0; c < n_cand; c++) names.push_back(cands[c].name);
+  const int forced = tune_forced(key, names);
+  if (forced >= 0) {
+    choice = forced;
+  } else if (ctx->autotune && !tune_get(key, &choice) && tune_allowed(ctx)) {
     // every run rebuilds F from Phi, so timing the candidates in place is
     // harmless; the chosen one runs last
     int rc = tune_pick(ctx, key, n_cand, names, [&](int c) { return pae_all(ctx, P, cands[c]); }, 2, &choice);

@@ -332,7 +332,10 @@ int launch_phir(tups_ctx* ctx) {
   if (fit.empty()) return set_error(ctx, TUPS_ERR_BADDIM, "k_phir: too many form-factor pairs for one CTA");
   int choice = 0;
   int rc = TUPS_OK;
-  if (ctx->autotune && !tune_get(key, &choice) && tune_allowed(ctx)) {
+  const int forced = tune_forced(key, names);
+  if (forced >= 0) {
+    choice = forced;
+  } else if (ctx->autotune && !tune_get(key, &choice) && tune_allowed(ctx)) {
     rc = tune_pick(ctx, key, (int)fit.size(), names, [&](int c) { return phir_run(ctx, P, fit[c]); }, 2, &choice);
     if (rc) return rc;
   }

@@ -29,7 +29,18 @@ struct TuneEntry {
 };
 std::mutex g_tune_mu;
 std::map<std::string, TuneEntry> g_tune;
+// candidates fixed by name for every key that starts with a prefix
+std::vector<std::pair<std::string, std::string>> g_force;
 }  // namespace
+
+int tune_forced(const std::string& key, const std::vector<std::string>& names) {
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  for (const auto& f : g_force)
+    if (key.compare(0, f.first.size(), f.first) == 0)
+      for (size_t c = 0; c < names.size(); c++)
+        if (names[c] == f.second) return (int)c;
+  return -1;
+}
 
 bool tune_get(const std::string& key, int* choice) {
   std::lock_guard<std::mutex> lock(g_tune_mu);
@@ -99,6 +110,22 @@ int tune_pick(tups_ctx* ctx, const std::string& key, int n_cand, const std::vect
 extern "C" int tups_set_autotune(tups_ctx* ctx, int enable) {
   if (!ctx) return TUPS_ERR_BADARG;
   ctx->autotune = enable != 0;
+  return TUPS_OK;
+}
+
+extern "C" int tups_set_tuning(const char* key_prefix, const char* name) {
+  std::lock_guard<std::mutex> lock(tups::g_tune_mu);
+  if (!key_prefix) {
+    tups::g_force.clear();
+    return TUPS_OK;
+  }
+  const std::string k(key_prefix);
+  for (size_t i = 0; i < tups::g_force.size(); i++)
+    if (tups::g_force[i].first == k) {
+      tups::g_force.erase(tups::g_force.begin() + i);
+      break;
+    }
+  if (name) tups::g_force.emplace_back(k, std::string(name));
   return TUPS_OK;
 }
 

@@ -227,6 +227,8 @@ int set_error(tups_ctx* ctx, int code, const std::string& msg);
 
 // tile-shape tuner, tune.cu: process-wide choices keyed by kernel and shape
 bool tune_get(const std::string& key, int* choice);
+// index in names of the candidate fixed by tups_set_tuning for key, or -1
+int tune_forced(const std::string& key, const std::vector<std::string>& names);
 // false when the context has tuning off or its stream is being captured
 bool tune_allowed(tups_ctx* ctx);
 // time run(c) for c = 0..n_cand-1 (best of reps, CUDA events on the

@@ -527,6 +527,17 @@ def _conv_dict(ci: tups_conv_info) -> dict:
     return d
 
 
+def set_tuning(key_prefix: str | None, name: str | None) -> None:
+    """Fix the tuner candidate ``name`` for every key starting with
+    ``key_prefix`` in this process (``name=None`` drops the prefix,
+    ``key_prefix=None`` drops all); candidates write the same bits."""
+    lib = _lib.load()
+    rc = lib.tups_set_tuning(None if key_prefix is None else key_prefix.encode(),
+                             None if name is None else name.encode())
+    if rc != 0:
+        raise RuntimeError(f"tups_set_tuning failed: {rc}")
+
+
 def tuning_table() -> list[str]:
     """The tile-shape tuner's choices in this process, one line per kernel
     and shape: ``key | choice NAME | NAME=ms ...``."""
