@@ -361,16 +361,18 @@ extern "C" int tups_iteration(tups_ctx* ctx, int ite, tups_conv_info* info) {
 // The device work of one iteration with no host synchronisation: Green's
 // function, BSE, Phi(R), parquet equation, SDE, the conv kernels,
 // SigmaOld = Sigma and the vertex update.  The output block only moves mu
-// and does not touch the vertices, so it follows the update on the host.
+// and does not touch the vertices, so it follows the update on the host;
+// the update does not change F, so max|F_r| is taken in the update's own
+// pass over F.
 static int iteration_device(tups_ctx* ctx, int slices, bool do_sde) {
   TRY(green_async(ctx, 0));
   TRY(bse_async(ctx, slices));
   TRY(tups::launch_phir(ctx));
   TRY(tups::launch_pae(ctx));
   if (do_sde) TRY(sde_async(ctx));
-  TRY(tups::launch_conv(ctx));
+  TRY(tups::launch_conv_sigma(ctx));
   TRY(copy_sigma_old(ctx));
-  return tups::launch_vertex_update(ctx);
+  return tups::launch_vertex_update_fmax(ctx);
 }
 
 // One iteration replayed from a CUDA graph captured on first use for each

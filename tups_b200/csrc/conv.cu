@@ -81,6 +81,31 @@ __global__ void k_vertex_update(cplx* __restrict__ G0, cplx* __restrict__ G1, cp
     G[i] = csub(F[i], G[i]);
 }
 
+// Both of the above in one pass over F: G_r = F_r - G_r, max |F_r| and the
+// NaN flag (k_conv_sigma has reset the maxima before it).  The maxima are
+// exact, so they do not depend on the order of the atomics.
+__global__ void k_vertex_update_fmax(cplx* __restrict__ G0, cplx* __restrict__ G1, cplx* __restrict__ G2,
+                                     cplx* __restrict__ G3, const cplx* __restrict__ F0,
+                                     const cplx* __restrict__ F1, const cplx* __restrict__ F2,
+                                     const cplx* __restrict__ F3, size_t n, double* scal) {
+  cplx* G = blockIdx.y == 0 ? G0 : (blockIdx.y == 1 ? G1 : (blockIdx.y == 2 ? G2 : G3));
+  const cplx* F = blockIdx.y == 0 ? F0 : (blockIdx.y == 1 ? F1 : (blockIdx.y == 2 ? F2 : F3));
+  double mx = 0.0, bad = 0.0;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const cplx v = F[i];
+    const double a2 = v.x * v.x + v.y * v.y;
+    if (!isfinite(a2)) bad = 1.0;
+    mx = fmax(mx, a2);
+    G[i] = csub(v, G[i]);
+  }
+  mx = warp_max(mx);
+  bad = warp_max(bad);
+  if ((threadIdx.x & 31) == 0) {
+    atomic_max_nonneg(&scal[S_FMAX + blockIdx.y], sqrt(mx));
+    if (bad > 0.0) atomic_max_nonneg(&scal[S_NANFLAG], 1.0);
+  }
+}
+
 // F = G = aux * Lambda(:, :, w) on the (l=1, l=1) nu-block of every slot, w
 // the slot's bosonic index (SRC/preprocessing.f90:102-116)
 __global__ void k_fill_lambda_block(cplx* __restrict__ F, cplx* __restrict__ G, const cplx* __restrict__ L,
@@ -122,10 +147,14 @@ int launch_set_l1_block(tups_ctx* ctx, cplx* G, double vr, double vi) {
   return after_launch(ctx, "k_set_l1_block");
 }
 
+int launch_conv_sigma(tups_ctx* ctx) {
+  k_conv_sigma<<<1, 1024, 0, ctx->stream>>>(ctx->s.Sigma, ctx->s.SigmaOld, ctx->s.scal, ctx->d.Nt);
+  return after_launch(ctx, "k_conv_sigma");
+}
+
 int launch_conv(tups_ctx* ctx) {
   const auto& d = ctx->d;
-  k_conv_sigma<<<1, 1024, 0, ctx->stream>>>(ctx->s.Sigma, ctx->s.SigmaOld, ctx->s.scal, d.Nt);
-  int rc = after_launch(ctx, "k_conv_sigma");
+  int rc = launch_conv_sigma(ctx);
   if (rc) return rc;
   const size_t n = (size_t)d.Nz * d.Nz * d.Nb;
   dim3 grid((unsigned)std::min<size_t>(cdiv(n, 256), 148 * 8), 4);
@@ -144,6 +173,18 @@ int launch_vertex_update(tups_ctx* ctx) {
   k_vertex_update<<<grid, 256, 0, ctx->stream>>>(ctx->s.G[0], ctx->s.G[1], ctx->s.G[2], ctx->s.G[3], ctx->s.F[0],
                                                  ctx->s.F[1], ctx->s.F[2], ctx->s.F[3], n);
   return after_launch(ctx, "k_vertex_update");
+}
+
+int launch_vertex_update_fmax(tups_ctx* ctx) {
+  const auto& d = ctx->d;
+  const size_t n = (size_t)d.Nz * d.Nz * d.Nb;
+  dim3 grid((unsigned)std::min<size_t>(cdiv(n, 256), 148 * 8), 4);
+  k_vertex_update_fmax<<<grid, 256, 0, ctx->stream>>>(ctx->s.G[0], ctx->s.G[1], ctx->s.G[2], ctx->s.G[3],
+                                                      ctx->s.F[0], ctx->s.F[1], ctx->s.F[2], ctx->s.F[3], n,
+                                                      ctx->s.scal);
+  int rc = after_launch(ctx, "k_vertex_update_fmax");
+  if (rc) return rc;
+  return exchange(ctx, TUPS_XCH_FMAX, ctx->s.scal + S_FMAX, 5, TUPS_XCH_MAX);
 }
 
 }  // namespace tups

@@ -261,6 +261,10 @@ int launch_pae(tups_ctx* ctx);
 int launch_sde(tups_ctx* ctx);
 int launch_conv(tups_ctx* ctx);
 int launch_vertex_update(tups_ctx* ctx);
+// k_conv_sigma alone, and the vertex update fused with max|F_r| (the rest
+// of launch_conv), for an iteration that runs both back to back
+int launch_conv_sigma(tups_ctx* ctx);
+int launch_vertex_update_fmax(tups_ctx* ctx);
 int launch_output_mu(tups_ctx* ctx);
 int launch_fft2d(tups_ctx* ctx, const cplx* in, cplx* out, int forward);
 int launch_chi_aux(tups_ctx* ctx);
