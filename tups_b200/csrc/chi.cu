@@ -125,13 +125,16 @@ __global__ void __launch_bounds__(256) k_chi_aux(const cplx* __restrict__ Sigma,
   }
 }
 
-// frequencies per CTA of the bubble kernels: at most 8 (several CTAs per
-// SM even at 8x8 / Nb = 240), the chunk's bubbles in at most 64 KB of
-// shared memory
+// frequencies per CTA of the bubble kernels: up to 8 on lattices of at
+// most 128 momenta (8x8: 0.059 -> 0.054 ms per call), one on larger ones,
+// where a CTA already has Nc bubbles to sum (16x16: 6.45 ms with one, 6.62
+// with two, 7.27 with eight per CTA); 128 threads for one, 256 for a chunk
 static int chi_chunk(int Nc, int nfreq) {
-  const int nc = std::max(1, (64 * 1024) / (2 * Nc * (int)sizeof(cplx)));
+  if (Nc > 128) return 1;
+  const int nc = std::max(1, (16 * 1024) / (2 * Nc * (int)sizeof(cplx)));
   return std::min(std::min(nc, 8), nfreq);
 }
+static int chi_threads(int nc) { return nc == 1 ? 128 : 256; }
 
 int launch_chi(tups_ctx* ctx, int q_begin, int q_count) {
   const auto& d = ctx->d;
@@ -142,7 +145,7 @@ int launch_chi(tups_ctx* ctx, int q_begin, int q_count) {
     cudaError_t e = cudaFuncSetAttribute(k_chi_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return cuda_check(ctx, e, "k_chi_blocks smem attribute");
   }
-  k_chi_blocks<<<grid, 256, sm, ctx->stream>>>(ctx->s.Sigma, ctx->s.SigmaH, ctx->t.Ekg, ctx->t.FF, ibz_local(ctx),
+  k_chi_blocks<<<grid, chi_threads(nc), sm, ctx->stream>>>(ctx->s.Sigma, ctx->s.SigmaH, ctx->t.Ekg, ctx->t.FF, ibz_local(ctx),
                                                ctx->s.scal, ctx->s.chi_ph, ctx->s.chi_pp, q_begin, d.Nx, d.Ny, d.Nf,
                                                d.Ngrain, d.Nl, ctx->p.beta, nc);
   return after_launch(ctx, "k_chi_blocks");
@@ -157,7 +160,7 @@ int launch_chi_aux(tups_ctx* ctx) {
     cudaError_t e = cudaFuncSetAttribute(k_chi_aux, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return cuda_check(ctx, e, "k_chi_aux smem attribute");
   }
-  k_chi_aux<<<grid, 256, sm, ctx->stream>>>(ctx->s.Sigma, ctx->s.SigmaH, ctx->t.Ekg, ctx->t.FF, ibz_local(ctx),
+  k_chi_aux<<<grid, chi_threads(nc), sm, ctx->stream>>>(ctx->s.Sigma, ctx->s.SigmaH, ctx->t.Ekg, ctx->t.FF, ibz_local(ctx),
                                             ctx->s.scal, ctx->s.chi_aux_ph, ctx->s.chi_aux_pp, d.Nx, d.Ny, d.Nf,
                                             d.Ngrain, d.Nl, ctx->p.f_range, ctx->p.beta, nc);
   return after_launch(ctx, "k_chi_aux");

@@ -181,6 +181,10 @@ __global__ void __launch_bounds__(32 * RW * WN, RW * WN == 8 ? (TN <= 2 ? PAE_MI
   cplx* sB = sX + (size_t)STG * 2 * PAE_BK * LDX;                             // [STG][BN][LDB]
   long long* koff = reinterpret_cast<long long*>(sB + (size_t)STG * BN * PAE_LDB);  // [Kpad]
   double* ksg = reinterpret_cast<double*>(koff + Kpad);                       // [Kpad]
+  // M^T offsets, split as (k part) + (column part); -1 marks a zero fill
+  // (M holds Nl^4 NIBZ NR < 2^31 entries: checked at launch)
+  int* bko = reinterpret_cast<int*>(ksg + Kpad);                              // [Kpad]
+  int* bco = bko + Kpad;                                                      // [BN]
   __shared__ long long e_off[E];
   __shared__ int e_ok[E], e_tr[E], e_nu1[E], e_nu2[E];
   __shared__ double fac[2][2];
@@ -241,6 +245,14 @@ __global__ void __launch_bounds__(32 * RW * WN, RW * WN == 8 ? (TN <= 2 ? PAE_MI
     }
     koff[k] = off;
     ksg[k] = sg;
+    bko[k] = k < K ? nl2 * (k % nl2) + nl4 * NIBZ * (k / nl2) : -1;
+  }
+  for (int n = tid; n < BN; n += NT) {
+    const int nn = col0 + n;
+    const int iq = QN == 1 ? 0 : nn / nl2;
+    const int col = nn - iq * nl2;
+    const bool ok = col < nl2 && (QN == 0 || iq < QN) && Q0 + iq <= Qhi;
+    bco[n] = ok ? col + nl4 * (Q0 + iq) : -1;
   }
   if (tid == 0) {
     // dispatch factors fac[source][target] of this family (SRC/parquet_EQOuter.f90:84-113)
@@ -272,17 +284,9 @@ __global__ void __launch_bounds__(32 * RW * WN, RW * WN == 8 ? (TN <= 2 ? PAE_MI
     cplx* dB = sB + (size_t)stage * BN * PAE_LDB;
     for (int p = tid; p < BN * PAE_BK; p += NT) {
       const int kk = p % PAE_BK, n = p / PAE_BK;
-      const int k = kt * PAE_BK + kk;
-      const int nn = col0 + n;
-      const int iq = QN == 1 ? 0 : nn / nl2;
-      const int col = nn - iq * nl2;
-      const bool ok = k < K && col < nl2 && (QN == 0 || iq < QN) && Q0 + iq <= Qhi;
-      const cplx* src = Mf;
-      if (ok) {
-        const int l34 = k % nl2, R = k / nl2;
-        src = Mf + col + (size_t)nl2 * l34 + (size_t)nl4 * (Q0 + iq + (size_t)NIBZ * R);
-      }
-      cp_async16p(dB + n * PAE_LDB + kk, src, ok);
+      const int bk = bko[kt * PAE_BK + kk], bc = bco[n];
+      const bool ok = bk >= 0 && bc >= 0;
+      cp_async16p(dB + n * PAE_LDB + kk, ok ? Mf + bk + bc : Mf, ok);
     }
     asm volatile("cp.async.commit_group;\n" ::);
   };
@@ -428,7 +432,7 @@ static int run_pae(tups_ctx* ctx, const PaePtrs& P, int nchunks, int fam, int ma
   const int K = d.Nl * d.Nl * d.NR;
   const int Kpad = (K + PAE_BK - 1) / PAE_BK * PAE_BK;
   const size_t sm = (size_t)(STG * 2 * PAE_BK * LDX + STG * BN * PAE_LDB) * sizeof(cplx) +
-                    (size_t)Kpad * (sizeof(long long) + sizeof(double));
+                    (size_t)Kpad * (sizeof(long long) + sizeof(double) + sizeof(int)) + (size_t)BN * sizeof(int);
   auto kern = k_pae_mma<TN, WN, RW, STG, QN, G3, PRE>;
   if (sm > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -560,6 +564,8 @@ int launch_pae(tups_ctx* ctx) {
   const auto& d = ctx->d;
   if (d.Nl > 13) return set_error(ctx, TUPS_ERR_BADDIM, "Nl > 13 not supported by the crossing kernel");
   if (d.Nf > 255) return set_error(ctx, TUPS_ERR_BADDIM, "Nf > 255 not supported by the crossing kernel");
+  if ((long long)d.Nl * d.Nl * d.Nl * d.Nl * d.NIBZ * d.NR >= (1LL << 31))
+    return set_error(ctx, TUPS_ERR_BADDIM, "crossing tensor too large for 32-bit offsets");
   if (!ctx->t.pae_elems) {
     int rc = build_pae_lists(ctx);
     if (rc) return rc;
