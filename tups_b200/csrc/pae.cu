@@ -44,6 +44,12 @@ struct PaePtrs {
 
 __host__ __device__ __forceinline__ int clampnu(int x, int Nf) { return x < 1 ? 1 : (x > Nf ? Nf : x); }
 
+// dispatch factors [pair][family][source][target] of SRC/parquet_EQOuter.f90:84-113:
+// pair 0: D = phbar_to_ph from (d, m), A = pp_to_ph from (s, t);
+// pair 1: D = phbar_to_pp from (d, m), A = ph_to_pp from (d, m)
+__constant__ double c_pae_fac[2][2][2][2] = {{{{-0.5, -0.5}, {-1.5, 0.5}}, {{0.5, -0.5}, {1.5, 0.5}}},
+                                             {{{0.5, -0.5}, {-1.5, -0.5}}, {{0.5, 0.5}, {-1.5, 0.5}}}};
+
 // Frequency map of family fam (0 = D, 1 = A) of target pair `pair` at the
 // element (nu1, nu2).  Returns false when the family does not reach it.
 __host__ __device__ __forceinline__ bool pae_family(int pair, int fam, int nu1, int nu2, int W, int Nf, int* w2,
@@ -131,16 +137,20 @@ __global__ void k_pae_base(PaePtrs P, const int* __restrict__ ibz, int Nz, int N
   const size_t n2 = (size_t)Nz * Nz;
   const size_t n = n2 * Nb;
   const int r = blockIdx.y;
+  // constant indices keep the parameter struct out of local memory
+  const cplx* Phi = r == 0 ? P.Phi[0] : r == 1 ? P.Phi[1] : r == 2 ? P.Phi[2] : P.Phi[3];
+  const cplx* L = r == 0 ? P.L[0] : r == 1 ? P.L[1] : r == 2 ? P.L[2] : P.L[3];
+  cplx* F = r == 0 ? P.F[0] : r == 1 ? P.F[1] : r == 2 ? P.F[2] : P.F[3];
   for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
-    cplx f = __ldcs(P.Phi[r] + e);
+    cplx f = __ldcs(Phi + e);
     const int i = (int)(e % Nz), j = (int)((e / Nz) % Nz);
     if (i < Nf && j < Nf) {
       const int q = (int)(e / n2);
       const int W = ibz[3 * q + 2];
-      const cplx lam = P.L[r][(size_t)i + (size_t)Nf * (j + (size_t)Nf * (W - 1))];
+      const cplx lam = L[(size_t)i + (size_t)Nf * (j + (size_t)Nf * (W - 1))];
       f = cadd(f, cscale(lam, aux));
     }
-    P.F[r][e] = f;
+    F[e] = f;
   }
 }
 
@@ -186,9 +196,9 @@ __global__ void __launch_bounds__(32 * RW * WN, RW * WN == 8 ? (TN <= 2 ? PAE_MI
   int* bko = reinterpret_cast<int*>(ksg + Kpad);                              // [Kpad]
   int* bco = bko + Kpad;                                                      // [BN]
   __shared__ long long e_off[E];
-  __shared__ int e_ok[E], e_tr[E], e_nu1[E], e_nu2[E];
-  __shared__ double fac[2][2];
-  __shared__ int src0;
+  __shared__ int e_ok[E], e_tr[E];
+  __shared__ int erow[E];        // output offset (nu1-1) + Nz (nu2-1), -1 past the list
+  __shared__ long long ecol[BN];  // output offset of column n (l1, l2, slot), -1 if not written
 
   // grid (Q, tile x pair x chunk, w): the CTAs in flight are the IBZ momenta of
   // one element tile, so they gather the same Phi(R) entries (Phi(R) does not
@@ -226,8 +236,7 @@ __global__ void __launch_bounds__(32 * RW * WN, RW * WN == 8 ? (TN <= 2 ? PAE_MI
     int4 rec = make_int4(0, 0, 1, 1);
     if (e0 + tid < cnt) rec = elems[(size_t)list * Nf * Nf + e0 + tid];
     const int w2 = rec.y, a = rec.z, b = rec.w & 65535;
-    e_nu1[tid] = rec.x & 255;
-    e_nu2[tid] = rec.x >> 8;
+    erow[tid] = e0 + tid < cnt ? ((rec.x & 255) - 1) + Nz * ((rec.x >> 8) - 1) : -1;
     e_ok[tid] = w2 != 0;
     e_tr[tid] = rec.w >> 16;
     // element part of the Phi(R) index (a-1) + Nz (b-1) + Nz^2 (w2-1)
@@ -253,22 +262,20 @@ __global__ void __launch_bounds__(32 * RW * WN, RW * WN == 8 ? (TN <= 2 ? PAE_MI
     const int col = nn - iq * nl2;
     const bool ok = col < nl2 && (QN == 0 || iq < QN) && Q0 + iq <= Qhi;
     bco[n] = ok ? col + nl4 * (Q0 + iq) : -1;
+    const int lq = col < nl2 ? local_slot(iq) : -1;
+    ecol[n] = lq >= 0 ? (long long)((col % Nl) * Nf) + (long long)Nz * ((col / Nl) * Nf) + (long long)n2 * lq : -1;
   }
-  if (tid == 0) {
-    // dispatch factors fac[source][target] of this family (SRC/parquet_EQOuter.f90:84-113)
-    // pair 0: D = phbar_to_ph from (d, m), A = pp_to_ph from (s, t)
-    // pair 1: D = phbar_to_pp from (d, m), A = ph_to_pp from (d, m)
-    const double f0[2][2][2] = {{{-0.5, -0.5}, {-1.5, 0.5}}, {{0.5, -0.5}, {1.5, 0.5}}};
-    const double f1[2][2][2] = {{{0.5, -0.5}, {-1.5, -0.5}}, {{0.5, 0.5}, {-1.5, 0.5}}};
-    for (int y = 0; y < 2; y++)
-      for (int z = 0; z < 2; z++) fac[y][z] = pair == 0 ? f0[fam][y][z] : f1[fam][y][z];
-    src0 = (fam == 1 && pair == 0) ? 2 : 0;
-  }
-  const cplx* Mf = P.M[pair == 0 ? (fam == 0 ? 0 : 1) : (fam == 0 ? 3 : 2)];
+  // dispatch factors fac[source][target] of this family (SRC/parquet_EQOuter.f90:84-113)
+  const double f00 = c_pae_fac[pair][fam][0][0], f01 = c_pae_fac[pair][fam][0][1];
+  const double f10 = c_pae_fac[pair][fam][1][0], f11 = c_pae_fac[pair][fam][1][1];
+  // constant indices keep the parameter struct out of local memory
+  const cplx* Mf = pair == 0 ? (fam == 0 ? P.M[0] : P.M[1]) : (fam == 0 ? P.M[3] : P.M[2]);
+  // sources: (d, m), except pp_to_ph from (s, t)
+  const bool st_src = fam == 1 && pair == 0;
+  const cplx* X0 = st_src ? P.PhiR[2] : P.PhiR[0];
+  const cplx* X1 = st_src ? P.PhiR[3] : P.PhiR[1];
   __syncthreads();
 
-  const cplx* X0 = P.PhiR[src0];
-  const cplx* X1 = P.PhiR[src0 + 1];
   // one K step: raw X (2 sources x BK x E) and M^T (BN x BK), zero-filled
   // outside K, past the list and for columns beyond Nl^2
   auto load_stage = [&](int stage, int kt) {
@@ -296,7 +303,7 @@ __global__ void __launch_bounds__(32 * RW * WN, RW * WN == 8 ? (TN <= 2 ? PAE_MI
   const int gid = lane >> 2, tig = lane & 3;
   const int tgt = (wr * 16) / E;            // the warp's target channel
   const int er = (wr * 16) % E + gid;       // its elements er and er + 8
-  const double fa = fac[0][tgt], fb = fac[1][tgt];
+  const double fa = tgt == 0 ? f00 : f01, fb = tgt == 0 ? f10 : f11;
   const bool tr0 = e_tr[er] != 0, tr1 = e_tr[er + 8] != 0;
   // four products: cre, cim; three: P1 in cre, P2 in cim, P3 in c3
   double cre[TN][4], cim[TN][4], c3[G3 ? TN : 1][4];
@@ -355,8 +362,8 @@ __global__ void __launch_bounds__(32 * RW * WN, RW * WN == 8 ? (TN <= 2 ? PAE_MI
         const cplx x0 = cX[kk * LDX + e], x1 = cX[(PAE_BK + kk) * LDX + e];
         const bool trv = e_tr[e] != 0;
         const double sg = ksg[kt * PAE_BK + kk];
-        cX[kk * LDX + e] = combine(x0, x1, fac[0][0], fac[1][0], trv, sg);
-        cX[(PAE_BK + kk) * LDX + e] = combine(x0, x1, fac[0][1], fac[1][1], trv, sg);
+        cX[kk * LDX + e] = combine(x0, x1, f00, f10, trv, sg);
+        cX[(PAE_BK + kk) * LDX + e] = combine(x0, x1, f01, f11, trv, sg);
       }
       __syncthreads();
     }
@@ -403,23 +410,18 @@ __global__ void __launch_bounds__(32 * RW * WN, RW * WN == 8 ? (TN <= 2 ? PAE_MI
 
   // epilogue: F_target += C / Nx on the listed elements (each element is in
   // a family's list once, so a pass writes it at most once)
+  cplx* Ft = pair == 0 ? (tgt == 0 ? P.F[0] : P.F[1]) : (tgt == 0 ? P.F[2] : P.F[3]);
+  const int rw0 = erow[er], rw1 = erow[er + 8];
 #pragma unroll
   for (int j = 0; j < TN; j++)
 #pragma unroll
     for (int x = 0; x < 4; x++) {
-      const int e = er + (x >= 2 ? 8 : 0);
-      const int nn = col0 + (wc * TN + j) * 8 + 2 * tig + (x & 1);
-      const int iq = QN == 1 ? 0 : nn / nl2;
-      const int col = nn - iq * nl2;
-      if (col >= nl2 || e0 + e >= cnt) continue;
-      const int lq = local_slot(iq);
-      if (lq < 0) continue;
-      const int nu1 = e_nu1[e], nu2 = e_nu2[e];
-      const int l1 = col % Nl, l2 = col / Nl;
-      const int r = (pair == 0 ? 0 : 2) + tgt;
-      const size_t idx = (size_t)(l1 * Nf + nu1 - 1) + (size_t)Nz * (l2 * Nf + nu2 - 1) + n2 * lq;
-      const cplx f = P.F[r][idx];
-      P.F[r][idx] = cmk(f.x + inv_nx * cre[j][x], f.y + inv_nx * cim[j][x]);
+      const int rw = x >= 2 ? rw1 : rw0;
+      const long long c = ecol[(wc * TN + j) * 8 + 2 * tig + (x & 1)];
+      if (rw < 0 || c < 0) continue;
+      cplx* f = Ft + c + rw;
+      const cplx v = *f;
+      *f = cmk(v.x + inv_nx * cre[j][x], v.y + inv_nx * cim[j][x]);
     }
 }
 
