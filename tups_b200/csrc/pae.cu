@@ -123,7 +123,10 @@ __device__ __forceinline__ void dmma_16x8x8(double* c, const double* a, const do
 #define PAE_MIN_BLOCKS 3  // CTAs per SM asked of ptxas for the 8-warp, <= 2 n-tile configs (2 beyond)
 #endif
 constexpr int PAE_BK = 16;
-constexpr int PAE_LDB = PAE_BK + 4;
+// M^T stage row pitch [k][n] in complex entries: BN + 2, so that a warp's
+// fragment reads (k = k8 + tig, n = .. + gid) fall in distinct banks and a
+// K row is copied by consecutive threads from consecutive columns of M
+__host__ __device__ constexpr int pae_ldn(int bn) { return bn + 2; }
 
 // Element lists: for target pair p, family f and bosonic index W the
 // elements (nu1, nu2) the family reaches, packed as int4
@@ -185,11 +188,12 @@ __global__ void __launch_bounds__(32 * RW * WN, RW * WN == 8 ? (TN <= 2 ? PAE_MI
   constexpr int NT = 32 * RW * WN;
   constexpr int E = 8 * RW;      // listed elements per CTA
   constexpr int LDX = E + 2;     // elements + pad
+  constexpr int LDN = pae_ldn(BN);
   static_assert(E % 16 == 0, "a warp's 16 rows must share one target");
   extern __shared__ __align__(16) unsigned char smraw[];
   cplx* sX = reinterpret_cast<cplx*>(smraw);                                  // [STG][2][BK][LDX]
-  cplx* sB = sX + (size_t)STG * 2 * PAE_BK * LDX;                             // [STG][BN][LDB]
-  long long* koff = reinterpret_cast<long long*>(sB + (size_t)STG * BN * PAE_LDB);  // [Kpad]
+  cplx* sB = sX + (size_t)STG * 2 * PAE_BK * LDX;                             // [STG][BK][LDN]
+  long long* koff = reinterpret_cast<long long*>(sB + (size_t)STG * PAE_BK * LDN);  // [Kpad]
   double* ksg = reinterpret_cast<double*>(koff + Kpad);                       // [Kpad]
   // M^T offsets, split as (k part) + (column part); -1 marks a zero fill
   // (M holds Nl^4 NIBZ NR < 2^31 entries: checked at launch)
@@ -288,12 +292,12 @@ __global__ void __launch_bounds__(32 * RW * WN, RW * WN == 8 ? (TN <= 2 ? PAE_MI
       const cplx* g = src ? X1 : X0;
       cp_async16p(dX + (src * PAE_BK + kk) * LDX + e, ok ? g + e_off[e] + koff[k] : g, ok);
     }
-    cplx* dB = sB + (size_t)stage * BN * PAE_LDB;
+    cplx* dB = sB + (size_t)stage * PAE_BK * LDN;
     for (int p = tid; p < BN * PAE_BK; p += NT) {
-      const int kk = p % PAE_BK, n = p / PAE_BK;
+      const int n = p % BN, kk = p / BN;
       const int bk = bko[kt * PAE_BK + kk], bc = bco[n];
       const bool ok = bk >= 0 && bc >= 0;
-      cp_async16p(dB + n * PAE_LDB + kk, ok ? Mf + bk + bc : Mf, ok);
+      cp_async16p(dB + kk * LDN + n, ok ? Mf + bk + bc : Mf, ok);
     }
     asm volatile("cp.async.commit_group;\n" ::);
   };
@@ -353,7 +357,7 @@ __global__ void __launch_bounds__(32 * RW * WN, RW * WN == 8 ? (TN <= 2 ? PAE_MI
       else asm volatile("cp.async.commit_group;\n" ::);
     }
     cplx* cX = sX + (size_t)(kt % STG) * 2 * PAE_BK * LDX;
-    const cplx* cB = sB + (size_t)(kt % STG) * BN * PAE_LDB;
+    const cplx* cB = sB + (size_t)(kt % STG) * PAE_BK * LDN;
     if (PRE) {
       // (source 0, source 1) at (k, e) -> (target 0, target 1) at (k, e):
       // each thread rewrites the entries it read
@@ -380,7 +384,7 @@ __global__ void __launch_bounds__(32 * RW * WN, RW * WN == 8 ? (TN <= 2 ? PAE_MI
 #pragma unroll
       for (int j = 0; j < TN; j++) {
         const int nb = (wc * TN + j) * 8 + gid;
-        const cplx w0 = cB[nb * PAE_LDB + k8 + tig], w1 = cB[nb * PAE_LDB + k8 + tig + 4];
+        const cplx w0 = cB[(k8 + tig) * LDN + nb], w1 = cB[(k8 + tig + 4) * LDN + nb];
         const double bre[2] = {w0.x, w1.x}, bim[2] = {w0.y, w1.y};
         if (G3) {
           const double bsum[2] = {w0.x + w0.y, w1.x + w1.y};
@@ -433,7 +437,7 @@ static int run_pae(tups_ctx* ctx, const PaePtrs& P, int nchunks, int fam, int ma
   constexpr int LDX = E + 2;
   const int K = d.Nl * d.Nl * d.NR;
   const int Kpad = (K + PAE_BK - 1) / PAE_BK * PAE_BK;
-  const size_t sm = (size_t)(STG * 2 * PAE_BK * LDX + STG * BN * PAE_LDB) * sizeof(cplx) +
+  const size_t sm = (size_t)(STG * 2 * PAE_BK * LDX + STG * PAE_BK * pae_ldn(BN)) * sizeof(cplx) +
                     (size_t)Kpad * (sizeof(long long) + sizeof(double) + sizeof(int)) + (size_t)BN * sizeof(int);
   auto kern = k_pae_mma<TN, WN, RW, STG, QN, G3, PRE>;
   if (sm > 48 * 1024) {
