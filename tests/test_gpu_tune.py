@@ -48,36 +48,40 @@ def test_tuned_tiles_equal_default_tiles(gpu_lib, case):
         assert float(ms[choice]) == min(float(v) for v in ms.values())
 
 
-@pytest.mark.parametrize("case,names", [
-    (dict(Nx=4, Nf=10, neighbours=2), ["g3_flat_bn32_tn2", "g3_flat_bn64_tn4", "g3_flat_bn48_tn3",
-                                       "g3_flat_bn32_tn2_s3", "g3_flat_bn48_tn3_s3", "g3p_flat_bn32_tn2",
-                                       "g3p_flat_bn64_tn4"]),
-    (dict(Nx=8, Nf=6, neighbours=3), ["g3_flat_bn64_tn4", "g3_flat_bn48_tn3", "g3_flat_bn32_tn2",
-                                      "g3_flat_bn48_tn3_s3", "g3_flat_bn32_tn2_s3", "g3p_flat_bn64_tn4",
-                                      "g3p_flat_bn48_tn3"]),
+@pytest.mark.parametrize("case", [
+    dict(Nx=4, Nf=10, neighbours=2),    # Nl = 5
+    dict(Nx=8, Nf=6, neighbours=3),     # Nl = 9
 ], ids=["nl5", "nl9"])
-def test_every_crossing_candidate_writes_the_same_bits(gpu_lib, case, names):
-    """Each three-product crossing candidate, fixed by name, against the
-    first: the same F after two full iterations and a third crossing."""
+def test_every_crossing_candidate_writes_the_same_bits(gpu_lib, case):
+    """Each three-product crossing candidate (names from the tuner's own
+    table), fixed by name, against the first: the same F after two full
+    iterations and a third crossing."""
     from tups_b200 import Params, Solver
-    from tups_b200.parquet import set_tuning
+    from tups_b200.parquet import set_tuning, tuning_table
     p = Params(beta=3.0, U=2.0, nParticle=0.95, f_damping=0.5, ite_max=10, **case)
-    ref = None
+
+    def crossing(name):
+        set_tuning("k_pae_mma(3M) ", name)
+        sol = Solver(p)
+        for ite in range(2):
+            sol.iteration(ite)
+        sol.calc_Gkw_Grt(2, False)
+        sol.BSE(2)
+        sol.calc_PhiR(2)
+        sol.calculate_PAE()
+        F = [sol.F(r) for r in "dmst"]
+        Nl = sol.Nl
+        sol.close()
+        return F, Nl
+
     try:
+        ref, Nl = crossing(None)     # tuned: fills the table with every candidate
+        line = [ln for ln in tuning_table() if ln.startswith(f"k_pae_mma(3M) Nl={Nl} Nf={p.Nf} ")]
+        assert line, tuning_table()
+        names = [kv.split("=")[0] for kv in line[0].split(" | ")[2].split()]
+        assert len(names) >= 4, names
         for name in names:
-            set_tuning("k_pae_mma(3M) ", name)
-            sol = Solver(p)
-            for ite in range(2):
-                sol.iteration(ite)
-            sol.calc_Gkw_Grt(2, False)
-            sol.BSE(2)
-            sol.calc_PhiR(2)
-            sol.calculate_PAE()
-            F = [sol.F(r) for r in "dmst"]
-            sol.close()
-            if ref is None:
-                ref = F
-                continue
+            F, _ = crossing(name)
             for r in range(4):
                 assert np.array_equal(F[r], ref[r]), (name, r)
     finally:

@@ -531,27 +531,25 @@ static const PaeCand kPaeWide[] = {
 };
 // three real products per complex one (Gauss): a different rounding of each
 // sum, so these form their own candidate set, chosen by the context's
-// crossing-products setting; the widths that fit 128 registers unspilled
-// (index 0: the tuner's pick on a B200 at 8x8 / Nl = 5, 1.560 ms against
-// 1.573 for 64 columns; at 16x16 / Nl = 9 64 columns won, 372 ms against
-// 392 for 48); three-stage pipelines at the widths that keep two CTAs per SM
+// crossing-products setting.  "g3p" candidates rewrite each landed X stage
+// as per-target operands (PRE); "_s3" ones run a three-stage pipeline.
+// Index 0 is the tuner's pick on a B200: at 8x8 / Nl = 5 64 flat columns
+// (1.35 ms against 1.37 for the PRE form on 32), at 16x16 / Nl = 9 the PRE
+// form on 64 columns (327 ms against 333 on 48 and 345 without PRE).
 static const PaeCand kPaeNl5G3[] = {
-    {"g3_flat_bn32_tn2", run_pae<2, 2, 4, 2, 0, true>, 32},
     {"g3_flat_bn64_tn4", run_pae<4, 2, 4, 2, 0, true>, 64},
-    {"g3_flat_bn48_tn3", run_pae<3, 2, 4, 2, 0, true>, 48},
-    {"g3_flat_bn32_tn2_s3", run_pae<2, 2, 4, 3, 0, true>, 32},
-    {"g3_flat_bn48_tn3_s3", run_pae<3, 2, 4, 3, 0, true>, 48},
     {"g3p_flat_bn32_tn2", run_pae<2, 2, 4, 2, 0, true, true>, 32},
+    {"g3_flat_bn48_tn3_s3", run_pae<3, 2, 4, 3, 0, true>, 48},
+    {"g3_flat_bn32_tn2", run_pae<2, 2, 4, 2, 0, true>, 32},
+    {"g3_flat_bn48_tn3", run_pae<3, 2, 4, 2, 0, true>, 48},
     {"g3p_flat_bn64_tn4", run_pae<4, 2, 4, 2, 0, true, true>, 64},
 };
 static const PaeCand kPaeWideG3[] = {
-    {"g3_flat_bn64_tn4", run_pae<4, 2, 4, 2, 0, true>, 64},
-    {"g3_flat_bn48_tn3", run_pae<3, 2, 4, 2, 0, true>, 48},
-    {"g3_flat_bn32_tn2", run_pae<2, 2, 4, 2, 0, true>, 32},
-    {"g3_flat_bn48_tn3_s3", run_pae<3, 2, 4, 3, 0, true>, 48},
-    {"g3_flat_bn32_tn2_s3", run_pae<2, 2, 4, 3, 0, true>, 32},
     {"g3p_flat_bn64_tn4", run_pae<4, 2, 4, 2, 0, true, true>, 64},
     {"g3p_flat_bn48_tn3", run_pae<3, 2, 4, 2, 0, true, true>, 48},
+    {"g3_flat_bn64_tn4", run_pae<4, 2, 4, 2, 0, true>, 64},
+    {"g3_flat_bn48_tn3", run_pae<3, 2, 4, 2, 0, true>, 48},
+    {"g3_flat_bn48_tn3_s3", run_pae<3, 2, 4, 3, 0, true>, 48},
 };
 
 static int pae_all(tups_ctx* ctx, const PaePtrs& P, const PaeCand& c) {
