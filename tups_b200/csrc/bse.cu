@@ -30,10 +30,13 @@ struct BsePtrs {
 // One row of CTAs per instance (blockIdx.y); every thread takes one line
 // (a grid-stride loop over all instances at a few CTAs per SM was slower at
 // 9 form factors: one line's loads in flight per thread).
+//
+// Gamma chi: the lanes of a warp run over rows at one nu, so every chi
+// entry they read is one address.
 template <int LMAX>
 __global__ void __launch_bounds__(256) k_bse_prep(BsePtrs P, const cplx* __restrict__ chi_ph,
-                                                  const cplx* __restrict__ chi_pp, cplx* __restrict__ A,
-                                                  cplx* __restrict__ B, int q_begin, int Nz, int Nf, int Nl) {
+                                                  const cplx* __restrict__ chi_pp, cplx* __restrict__ A, int q_begin,
+                                                  int Nz, int Nf, int Nl) {
   const size_t lines = (size_t)Nz * Nf;
   const int inst = blockIdx.y;
   const int q = q_begin + inst / 4, r = inst % 4;
@@ -42,37 +45,63 @@ __global__ void __launch_bounds__(256) k_bse_prep(BsePtrs P, const cplx* __restr
   const cplx* Gr = r == 0 ? P.G[0] : r == 1 ? P.G[1] : r == 2 ? P.G[2] : P.G[3];
   const cplx* Gm = Gr + (size_t)Nz * Nz * q;
   cplx* Ai = A + (size_t)Nz * Nz * inst;
-  cplx* Bi = B + (size_t)Nz * Nz * inst;
-  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < 2 * lines; t += (size_t)gridDim.x * blockDim.x) {
+  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < lines; t += (size_t)gridDim.x * blockDim.x) {
     cplx g[LMAX];
-    if (t < lines) {
-      // A[row, (l2, nu)] = sum_l1 Gamma[row, (l1, nu)] chi[l1, l2, nu]
-      const int row = (int)(t % Nz), nu = (int)(t / Nz);
+    // A[row, (l2, nu)] = sum_l1 Gamma[row, (l1, nu)] chi[l1, l2, nu]
+    const int row = (int)(t % Nz), nu = (int)(t / Nz);
 #pragma unroll
-      for (int l = 0; l < LMAX; l++)
-        if (l < Nl) g[l] = Gm[row + (size_t)Nz * (l * Nf + nu)];
-      for (int l2 = 0; l2 < Nl; l2++) {
-        cplx acc = cmk(0.0, 0.0);
+    for (int l = 0; l < LMAX; l++)
+      if (l < Nl) g[l] = Gm[row + (size_t)Nz * (l * Nf + nu)];
+    for (int l2 = 0; l2 < Nl; l2++) {
+      cplx acc = cmk(0.0, 0.0);
 #pragma unroll
-        for (int l1 = 0; l1 < LMAX; l1++)
-          if (l1 < Nl) acc = cfma(g[l1], chi[l1 + Nl * (l2 + (size_t)Nl * nu)], acc);
-        Ai[row + (size_t)Nz * (l2 * Nf + nu)] = acc;
-      }
-    } else {
-      // B[(l1, nu), col] = sum_l2 chi[l1, l2, nu] Gamma[(l2, nu), col]
-      const size_t u = t - lines;
-      const int nu = (int)(u % Nf), col = (int)(u / Nf);
-#pragma unroll
-      for (int l = 0; l < LMAX; l++)
-        if (l < Nl) g[l] = Gm[(l * Nf + nu) + (size_t)Nz * col];
-      for (int l1 = 0; l1 < Nl; l1++) {
-        cplx acc = cmk(0.0, 0.0);
-#pragma unroll
-        for (int l2 = 0; l2 < LMAX; l2++)
-          if (l2 < Nl) acc = cfma(chi[l1 + Nl * (l2 + (size_t)Nl * nu)], g[l2], acc);
-        Bi[(l1 * Nf + nu) + (size_t)Nz * col] = acc;
-      }
+      for (int l1 = 0; l1 < LMAX; l1++)
+        if (l1 < Nl) acc = cfma(g[l1], chi[l1 + Nl * (l2 + (size_t)Nl * nu)], acc);
+      Ai[row + (size_t)Nz * (l2 * Nf + nu)] = acc;
     }
+  }
+}
+
+// chi Gamma: B[(l1, nu), col] = sum_l2 chi[l1, l2, nu] Gamma[(l2, nu), col]
+// (sum in l2 ascending).  CTA = 32 frequencies (lanes) x 8 columns (warps)
+// of one instance; the lanes' chi entries differ in nu, so the CTA first
+// stages chi[:, :, nu0 .. nu0 + 31] in shared memory, [l1 + Nl l2][lane]
+// with a row pitch of 33 (conflict-free stores of consecutive l1 + Nl l2)
+// (read straight from global memory they were 32 cache lines per load).
+// Dynamic shared memory: Nl^2 x 33 complex.
+template <int LMAX>
+__global__ void __launch_bounds__(256) k_bse_prep_b(BsePtrs P, const cplx* __restrict__ chi_ph,
+                                                    const cplx* __restrict__ chi_pp, cplx* __restrict__ B, int q_begin,
+                                                    int Nz, int Nf, int Nl) {
+  extern __shared__ cplx chs[];  // [Nl * Nl][33]
+  const int inst = blockIdx.y;
+  const int q = q_begin + inst / 4, r = inst % 4;
+  const int nchunk = (Nf + 31) / 32;
+  const int nu0 = (blockIdx.x % nchunk) * 32, col = (blockIdx.x / nchunk) * 8 + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31, nu = nu0 + lane;
+  const int nl2 = Nl * Nl;
+  const cplx* chi = (r < 2 ? chi_ph : chi_pp) + (size_t)nl2 * Nf * q;
+  const int nn = min(32, Nf - nu0);
+  // chi[:, :, nu0 .. nu0 + nn) is contiguous in global memory
+  for (int e = threadIdx.x; e < nl2 * nn; e += blockDim.x) {
+    const int ll = e % nl2, j = e / nl2;
+    chs[ll * 33 + j] = chi[(size_t)ll + (size_t)nl2 * (nu0 + j)];
+  }
+  __syncthreads();
+  if (nu >= Nf || col >= Nz) return;
+  const cplx* Gr = r == 0 ? P.G[0] : r == 1 ? P.G[1] : r == 2 ? P.G[2] : P.G[3];
+  const cplx* Gm = Gr + (size_t)Nz * Nz * q + (size_t)Nz * col;
+  cplx* Bi = B + (size_t)Nz * Nz * inst + (size_t)Nz * col;
+  cplx g[LMAX];
+#pragma unroll
+  for (int l = 0; l < LMAX; l++)
+    if (l < Nl) g[l] = Gm[l * Nf + nu];
+  for (int l1 = 0; l1 < Nl; l1++) {
+    cplx acc = cmk(0.0, 0.0);
+#pragma unroll
+    for (int l2 = 0; l2 < LMAX; l2++)
+      if (l2 < Nl) acc = cfma(chs[(l1 + Nl * l2) * 33 + lane], g[l2], acc);
+    Bi[l1 * Nf + nu] = acc;
   }
 }
 
@@ -461,14 +490,28 @@ int launch_bse_chunk(tups_ctx* ctx, int q_begin, int q_count) {
   const int slices = ctx->cur_slices;
   if (d.Nl > 16) return set_error(ctx, TUPS_ERR_BADDIM, "Nl > 16 not supported by k_bse_prep");
   if (4 * q_count > 65535) return set_error(ctx, TUPS_ERR_BADDIM, "k_bse_prep: more than 16383 slots in a chunk");
-  const size_t lines2 = (size_t)2 * d.Nz * d.Nf;
-  const dim3 pgrid((unsigned)std::min<size_t>(cdiv(lines2, 256), 4096), 4 * q_count);
+  const size_t lines = (size_t)d.Nz * d.Nf;
+  const dim3 pgrid((unsigned)std::min<size_t>(cdiv(lines, 256), 4096), 4 * q_count);
   phase_begin(ctx, TUPS_PHASE_BSE_PREP);
   auto prep = d.Nl <= 1 ? k_bse_prep<1> : d.Nl <= 5 ? k_bse_prep<5> : d.Nl <= 9 ? k_bse_prep<9>
              : d.Nl <= 13 ? k_bse_prep<13> : k_bse_prep<16>;
-  prep<<<pgrid, 256, 0, ctx->stream>>>(P, ctx->s.chi_ph, ctx->s.chi_pp, ctx->s.bse_A, ctx->s.bse_B, q_begin, d.Nz,
-                                       d.Nf, d.Nl);
+  prep<<<pgrid, 256, 0, ctx->stream>>>(P, ctx->s.chi_ph, ctx->s.chi_pp, ctx->s.bse_A, q_begin, d.Nz, d.Nf, d.Nl);
   int rc = after_launch(ctx, "k_bse_prep");
+  if (!rc) {
+    auto prep_b = d.Nl <= 1 ? k_bse_prep_b<1> : d.Nl <= 5 ? k_bse_prep_b<5> : d.Nl <= 9 ? k_bse_prep_b<9>
+                 : d.Nl <= 13 ? k_bse_prep_b<13> : k_bse_prep_b<16>;
+    const size_t smb = (size_t)d.Nl * d.Nl * 33 * sizeof(cplx);
+    if (smb > 48 * 1024) {
+      cudaError_t e = cudaFuncSetAttribute(prep_b, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smb);
+      if (e != cudaSuccess) rc = cuda_check(ctx, e, "k_bse_prep_b smem attribute");
+    }
+    const dim3 bgrid((unsigned)(cdiv(d.Nf, 32) * cdiv(d.Nz, 8)), 4 * q_count);
+    if (!rc) {
+      prep_b<<<bgrid, 256, smb, ctx->stream>>>(P, ctx->s.chi_ph, ctx->s.chi_pp, ctx->s.bse_B, q_begin, d.Nz, d.Nf,
+                                               d.Nl);
+      rc = after_launch(ctx, "k_bse_prep_b");
+    }
+  }
   phase_end(ctx, TUPS_PHASE_BSE_PREP);
   if (rc) return rc;
   if (slices > 0) {
