@@ -25,8 +25,9 @@ struct PhirPtrs {
 // Phi[(a, nu_i), (b, nu_j), Q].  A CTA owns one nu_j, a tile of PH_TI
 // consecutive nu_i and one (w, r).  For each momentum Q of the context it
 // stages Phi[(a, nu_i), (b, nu_j), (Q, w)] for all a, b and the tile's nu_i
-// (Nl^2 runs of PH_TI contiguous complex) in shared memory, double buffered
-// with cp.async, and every symmetric image of Q reads its permuted entries
+// (Nl^2 runs of PH_TI contiguous complex) in shared memory with cp.async
+// (three buffers, copies two momenta ahead, one barrier per momentum), and
+// every symmetric image of Q reads its permuted entries
 // (lsym(l_i), lsym(l_j)) from there: each Phi(Q) element leaves HBM once and
 // the inner loop is FP64 FMAs on shared-memory operands.  Per output the sum
 // runs over Q ascending and, within Q, over the star's symmetries ascending.
@@ -35,6 +36,7 @@ struct PhirPtrs {
 // outputs nu_i = nu_i0 + c + SUB k, all NR lattice vectors; the phases
 // expSqR(Q, R, sym) of the star pairs sit in shared memory, packed by pair.
 constexpr int PH_TI = 16;
+constexpr int PH_STAGES = 3;  // Phi(Q) stages in shared memory (momenta in flight)
 
 __device__ __forceinline__ void ph_cp_async16(void* sdst, const void* gsrc, bool valid) {
   const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(sdst));
@@ -73,8 +75,8 @@ __global__ void __launch_bounds__(phir_max_threads(OPT, NR)) k_phir(PhirPtrs P, 
   constexpr int SUB = PH_TI / OPT;
   extern __shared__ __align__(16) unsigned char phir_sm[];
   const int nl2 = Nl * Nl;
-  cplx* sPhi = reinterpret_cast<cplx*>(phir_sm);          // [2][nl2][PH_TI]
-  cplx* sE = sPhi + (size_t)2 * nl2 * PH_TI;               // [npairs][NR]
+  cplx* sPhi = reinterpret_cast<cplx*>(phir_sm);          // [PH_STAGES][nl2][PH_TI]
+  cplx* sE = sPhi + (size_t)PH_STAGES * nl2 * PH_TI;       // [npairs][NR]
   int* sSym = reinterpret_cast<int*>(sE + (size_t)npairs * NR);  // [npairs] symmetry of pair p
   int* sBeg = sSym + npairs;                               // [NIBZ + 1] first pair of Q
   int* sQ = sBeg + NIBZ + 1;                               // [NIBZ] momenta of this context at w
@@ -157,16 +159,26 @@ __global__ void __launch_bounds__(phir_max_threads(OPT, NR)) k_phir(PhirPtrs P, 
   const cplx* G = r == 0 ? P.G[0] : r == 1 ? P.G[1] : r == 2 ? P.G[2] : P.G[3];
   const int stage_elems = nl2 * PH_TI;
   const cplx* Gw = G + (size_t)Nz * nj;  // element (0, (0, nj)); column (b, nj) is Nz Nf b further
-  if (nq > 0) ph_stage(sPhi, Gw + n2 * (size_t)(sQ[0] * nh + w - slot0), stage_elems, Nl, Nf, Nz, ni0);
-  asm volatile("cp.async.commit_group;\n" ::);
-  for (int qi = 0; qi < nq; qi++) {
-    if (qi + 1 < nq)
-      ph_stage(sPhi + (size_t)((qi + 1) & 1) * stage_elems, Gw + n2 * (size_t)(sQ[qi + 1] * nh + w - slot0),
-               stage_elems, Nl, Nf, Nz, ni0);
+  // three buffers, momenta staged two ahead: the barrier at the top of an
+  // iteration both publishes this momentum's stage and ends every read of
+  // the buffer the next copy overwrites, so one barrier per momentum
+#pragma unroll
+  for (int qq = 0; qq < PH_STAGES - 1; qq++) {
+    if (qq < nq) ph_stage(sPhi + (size_t)qq * stage_elems, Gw + n2 * (size_t)(sQ[qq] * nh + w - slot0), stage_elems,
+                          Nl, Nf, Nz, ni0);
     asm volatile("cp.async.commit_group;\n" ::);
-    asm volatile("cp.async.wait_group 1;\n" ::);
+  }
+  for (int qi = 0; qi < nq; qi++) {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(PH_STAGES - 2));
     __syncthreads();
-    const cplx* S = sPhi + (size_t)(qi & 1) * stage_elems;
+    {
+      const int qn = qi + PH_STAGES - 1;
+      if (qn < nq)
+        ph_stage(sPhi + (size_t)(qn % PH_STAGES) * stage_elems, Gw + n2 * (size_t)(sQ[qn] * nh + w - slot0),
+                 stage_elems, Nl, Nf, Nz, ni0);
+      asm volatile("cp.async.commit_group;\n" ::);
+    }
+    const cplx* S = sPhi + (size_t)(qi % PH_STAGES) * stage_elems;
     const int Q = sQ[qi];
     const int pe = sBeg[Q + 1];
     for (int pp = sBeg[Q]; pp < pe; pp++) {
@@ -188,7 +200,6 @@ __global__ void __launch_bounds__(phir_max_threads(OPT, NR)) k_phir(PhirPtrs P, 
         }
       }
     }
-    __syncthreads();
   }
   asm volatile("cp.async.wait_group 0;\n" ::);
   if (!active) return;
@@ -294,7 +305,7 @@ static int phir_run(tups_ctx* ctx, const PhirPtrs& P, int cand) {
   const int nl2 = d.Nl * d.Nl;
   const int threads = phir_threads(ctx, cand);
   if (!phir_fits(ctx, cand)) return set_error(ctx, TUPS_ERR_BADDIM, "k_phir: too many form-factor pairs for one CTA");
-  const size_t sm = (size_t)2 * nl2 * PH_TI * sizeof(cplx) + (size_t)npairs * d.NR * sizeof(cplx) +
+  const size_t sm = (size_t)PH_STAGES * nl2 * PH_TI * sizeof(cplx) + (size_t)npairs * d.NR * sizeof(cplx) +
                     ((size_t)npairs + 2 * d.NIBZ + 1) * sizeof(int);
   if (sm > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
