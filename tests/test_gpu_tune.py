@@ -86,3 +86,26 @@ def test_every_crossing_candidate_writes_the_same_bits(gpu_lib, case):
                 assert np.array_equal(F[r], ref[r]), (name, r)
     finally:
         set_tuning(None, None)
+
+
+def test_bse_prep_forms_write_the_same_bits(gpu_lib):
+    """The BSE prep as two launches or as one (a tuner choice) gives the
+    same vertices after two iterations."""
+    from tups_b200 import Params, Solver
+    from tups_b200.parquet import set_tuning
+    p = Params(beta=3.0, U=2.0, nParticle=0.95, f_damping=0.5, ite_max=10, Nx=8, Nf=6, neighbours=3)
+    out = {}
+    try:
+        for form in ("two_launches", "one_launch"):
+            set_tuning("k_bse_prep ", form)
+            sol = Solver(p)
+            for ite in range(2):
+                sol.iteration(ite)
+            out[form] = (sol.Sigma, [sol.G(r) for r in "dmst"])
+            sol.close()
+    finally:
+        set_tuning(None, None)
+    a, b = out["two_launches"], out["one_launch"]
+    assert np.array_equal(a[0], b[0])
+    for r in range(4):
+        assert np.array_equal(a[1][r], b[1][r]), r

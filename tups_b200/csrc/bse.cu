@@ -34,9 +34,9 @@ struct BsePtrs {
 // Gamma chi: the lanes of a warp run over rows at one nu, so every chi
 // entry they read is one address.
 template <int LMAX>
-__global__ void __launch_bounds__(256) k_bse_prep(BsePtrs P, const cplx* __restrict__ chi_ph,
-                                                  const cplx* __restrict__ chi_pp, cplx* __restrict__ A, int q_begin,
-                                                  int Nz, int Nf, int Nl) {
+__device__ __forceinline__ void prep_gamma_chi(const BsePtrs& P, const cplx* __restrict__ chi_ph,
+                                               const cplx* __restrict__ chi_pp, cplx* __restrict__ A, int q_begin,
+                                               int Nz, int Nf, int Nl, int cta, int ncta) {
   const size_t lines = (size_t)Nz * Nf;
   const int inst = blockIdx.y;
   const int q = q_begin + inst / 4, r = inst % 4;
@@ -45,7 +45,7 @@ __global__ void __launch_bounds__(256) k_bse_prep(BsePtrs P, const cplx* __restr
   const cplx* Gr = r == 0 ? P.G[0] : r == 1 ? P.G[1] : r == 2 ? P.G[2] : P.G[3];
   const cplx* Gm = Gr + (size_t)Nz * Nz * q;
   cplx* Ai = A + (size_t)Nz * Nz * inst;
-  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < lines; t += (size_t)gridDim.x * blockDim.x) {
+  for (size_t t = (size_t)cta * blockDim.x + threadIdx.x; t < lines; t += (size_t)ncta * blockDim.x) {
     cplx g[LMAX];
     // A[row, (l2, nu)] = sum_l1 Gamma[row, (l1, nu)] chi[l1, l2, nu]
     const int row = (int)(t % Nz), nu = (int)(t / Nz);
@@ -68,16 +68,15 @@ __global__ void __launch_bounds__(256) k_bse_prep(BsePtrs P, const cplx* __restr
 // stages chi[:, :, nu0 .. nu0 + 31] in shared memory, [l1 + Nl l2][lane]
 // with a row pitch of 33 (conflict-free stores of consecutive l1 + Nl l2)
 // (read straight from global memory they were 32 cache lines per load).
-// Dynamic shared memory: Nl^2 x 33 complex.
+// Shared memory chs: Nl^2 x 33 complex.
 template <int LMAX>
-__global__ void __launch_bounds__(256) k_bse_prep_b(BsePtrs P, const cplx* __restrict__ chi_ph,
-                                                    const cplx* __restrict__ chi_pp, cplx* __restrict__ B, int q_begin,
-                                                    int Nz, int Nf, int Nl) {
-  extern __shared__ cplx chs[];  // [Nl * Nl][33]
+__device__ __forceinline__ void prep_chi_gamma(const BsePtrs& P, const cplx* __restrict__ chi_ph,
+                                               const cplx* __restrict__ chi_pp, cplx* __restrict__ B, int q_begin,
+                                               int Nz, int Nf, int Nl, int cta, cplx* chs) {
   const int inst = blockIdx.y;
   const int q = q_begin + inst / 4, r = inst % 4;
   const int nchunk = (Nf + 31) / 32;
-  const int nu0 = (blockIdx.x % nchunk) * 32, col = (blockIdx.x / nchunk) * 8 + (threadIdx.x >> 5);
+  const int nu0 = (cta % nchunk) * 32, col = (cta / nchunk) * 8 + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31, nu = nu0 + lane;
   const int nl2 = Nl * Nl;
   const cplx* chi = (r < 2 ? chi_ph : chi_pp) + (size_t)nl2 * Nf * q;
@@ -103,6 +102,33 @@ __global__ void __launch_bounds__(256) k_bse_prep_b(BsePtrs P, const cplx* __res
       if (l2 < Nl) acc = cfma(chs[(l1 + Nl * l2) * 33 + lane], g[l2], acc);
     Bi[l1 * Nf + nu] = acc;
   }
+}
+
+// the two halves as separate launches (Gamma chi, then chi Gamma) ...
+template <int LMAX>
+__global__ void __launch_bounds__(256) k_bse_prep(BsePtrs P, const cplx* __restrict__ chi_ph,
+                                                  const cplx* __restrict__ chi_pp, cplx* __restrict__ A, int q_begin,
+                                                  int Nz, int Nf, int Nl) {
+  prep_gamma_chi<LMAX>(P, chi_ph, chi_pp, A, q_begin, Nz, Nf, Nl, blockIdx.x, gridDim.x);
+}
+template <int LMAX>
+__global__ void __launch_bounds__(256) k_bse_prep_b(BsePtrs P, const cplx* __restrict__ chi_ph,
+                                                    const cplx* __restrict__ chi_pp, cplx* __restrict__ B, int q_begin,
+                                                    int Nz, int Nf, int Nl) {
+  extern __shared__ cplx chs[];
+  prep_chi_gamma<LMAX>(P, chi_ph, chi_pp, B, q_begin, Nz, Nf, Nl, blockIdx.x, chs);
+}
+// ... or as one: the first nA CTAs of an instance's row form Gamma chi, the
+// rest chi Gamma, so the instance's Gamma, read by the first, is still in L2
+// for the second
+template <int LMAX>
+__global__ void __launch_bounds__(256) k_bse_prep_ab(BsePtrs P, const cplx* __restrict__ chi_ph,
+                                                     const cplx* __restrict__ chi_pp, cplx* __restrict__ A,
+                                                     cplx* __restrict__ B, int q_begin, int Nz, int Nf, int Nl,
+                                                     int nA) {
+  extern __shared__ cplx chs[];
+  if ((int)blockIdx.x < nA) prep_gamma_chi<LMAX>(P, chi_ph, chi_pp, A, q_begin, Nz, Nf, Nl, blockIdx.x, nA);
+  else prep_chi_gamma<LMAX>(P, chi_ph, chi_pp, B, q_begin, Nz, Nf, Nl, blockIdx.x - nA, chs);
 }
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
@@ -477,6 +503,63 @@ static int run_split(tups_ctx* ctx, const BsePtrs& P, int q_begin, int q_count, 
   return TUPS_OK;
 }
 
+// BSE prep launch forms (same bits): 0 = two launches, 1 = one launch
+static int prep_run(tups_ctx* ctx, const BsePtrs& P, int q_begin, int q_count, int form) {
+  const auto& d = ctx->d;
+  const int nA = (int)std::min<size_t>(cdiv((size_t)d.Nz * d.Nf, 256), 4096);
+  const int nB = (int)(cdiv(d.Nf, 32) * cdiv(d.Nz, 8));
+  const size_t smb = (size_t)d.Nl * d.Nl * 33 * sizeof(cplx);
+  const int L = d.Nl <= 1 ? 1 : d.Nl <= 5 ? 5 : d.Nl <= 9 ? 9 : d.Nl <= 13 ? 13 : 16;
+  auto attr = [&](const void* fn) {
+    if (smb <= 48 * 1024) return TUPS_OK;
+    return cuda_check(ctx, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smb),
+                      "k_bse_prep smem attribute");
+  };
+  if (form == 1) {
+    auto ab = L == 1 ? k_bse_prep_ab<1> : L == 5 ? k_bse_prep_ab<5> : L == 9 ? k_bse_prep_ab<9>
+            : L == 13 ? k_bse_prep_ab<13> : k_bse_prep_ab<16>;
+    int rc = attr((const void*)ab);
+    if (rc) return rc;
+    ab<<<dim3(nA + nB, 4 * q_count), 256, smb, ctx->stream>>>(P, ctx->s.chi_ph, ctx->s.chi_pp, ctx->s.bse_A,
+                                                               ctx->s.bse_B, q_begin, d.Nz, d.Nf, d.Nl, nA);
+    return after_launch(ctx, "k_bse_prep_ab");
+  }
+  auto pa = L == 1 ? k_bse_prep<1> : L == 5 ? k_bse_prep<5> : L == 9 ? k_bse_prep<9>
+          : L == 13 ? k_bse_prep<13> : k_bse_prep<16>;
+  pa<<<dim3(nA, 4 * q_count), 256, 0, ctx->stream>>>(P, ctx->s.chi_ph, ctx->s.chi_pp, ctx->s.bse_A, q_begin, d.Nz,
+                                                      d.Nf, d.Nl);
+  int rc = after_launch(ctx, "k_bse_prep");
+  if (rc) return rc;
+  auto pb = L == 1 ? k_bse_prep_b<1> : L == 5 ? k_bse_prep_b<5> : L == 9 ? k_bse_prep_b<9>
+          : L == 13 ? k_bse_prep_b<13> : k_bse_prep_b<16>;
+  rc = attr((const void*)pb);
+  if (rc) return rc;
+  pb<<<dim3(nB, 4 * q_count), 256, smb, ctx->stream>>>(P, ctx->s.chi_ph, ctx->s.chi_pp, ctx->s.bse_B, q_begin, d.Nz,
+                                                        d.Nf, d.Nl);
+  return after_launch(ctx, "k_bse_prep_b");
+}
+
+// Gamma chi and chi Gamma for one chunk; the launch form is a tuner choice
+// per shape, timed on the first chunk's own operands (the prep writes only
+// the scratch A and B, so running it more than once is harmless)
+static int prep_chunk(tups_ctx* ctx, const BsePtrs& P, int q_begin, int q_count) {
+  const auto& d = ctx->d;
+  if (d.Nl > 16) return set_error(ctx, TUPS_ERR_BADDIM, "Nl > 16 not supported by k_bse_prep");
+  if (4 * q_count > 65535) return set_error(ctx, TUPS_ERR_BADDIM, "k_bse_prep: more than 16383 slots in a chunk");
+  const std::string key = "k_bse_prep Nz=" + std::to_string(d.Nz) + " Nl=" + std::to_string(d.Nl);
+  const std::vector<std::string> names = {"two_launches", "one_launch"};
+  int choice = 0;
+  const int forced = tune_forced(key, names);
+  if (forced >= 0) {
+    choice = forced;
+  } else if (ctx->autotune && !tune_get(key, &choice) && q_begin == 0 && tune_allowed(ctx)) {
+    int rc = tune_pick(ctx, key, (int)names.size(), names,
+                       [&](int c) { return prep_run(ctx, P, q_begin, q_count, c); }, 2, &choice);
+    if (rc) return rc;
+  }
+  return prep_run(ctx, P, q_begin, q_count, choice);
+}
+
 int launch_bse_chunk(tups_ctx* ctx, int q_begin, int q_count) {
   const auto& d = ctx->d;
   BsePtrs P;
@@ -490,28 +573,8 @@ int launch_bse_chunk(tups_ctx* ctx, int q_begin, int q_count) {
   const int slices = ctx->cur_slices;
   if (d.Nl > 16) return set_error(ctx, TUPS_ERR_BADDIM, "Nl > 16 not supported by k_bse_prep");
   if (4 * q_count > 65535) return set_error(ctx, TUPS_ERR_BADDIM, "k_bse_prep: more than 16383 slots in a chunk");
-  const size_t lines = (size_t)d.Nz * d.Nf;
-  const dim3 pgrid((unsigned)std::min<size_t>(cdiv(lines, 256), 4096), 4 * q_count);
   phase_begin(ctx, TUPS_PHASE_BSE_PREP);
-  auto prep = d.Nl <= 1 ? k_bse_prep<1> : d.Nl <= 5 ? k_bse_prep<5> : d.Nl <= 9 ? k_bse_prep<9>
-             : d.Nl <= 13 ? k_bse_prep<13> : k_bse_prep<16>;
-  prep<<<pgrid, 256, 0, ctx->stream>>>(P, ctx->s.chi_ph, ctx->s.chi_pp, ctx->s.bse_A, q_begin, d.Nz, d.Nf, d.Nl);
-  int rc = after_launch(ctx, "k_bse_prep");
-  if (!rc) {
-    auto prep_b = d.Nl <= 1 ? k_bse_prep_b<1> : d.Nl <= 5 ? k_bse_prep_b<5> : d.Nl <= 9 ? k_bse_prep_b<9>
-                 : d.Nl <= 13 ? k_bse_prep_b<13> : k_bse_prep_b<16>;
-    const size_t smb = (size_t)d.Nl * d.Nl * 33 * sizeof(cplx);
-    if (smb > 48 * 1024) {
-      cudaError_t e = cudaFuncSetAttribute(prep_b, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smb);
-      if (e != cudaSuccess) rc = cuda_check(ctx, e, "k_bse_prep_b smem attribute");
-    }
-    const dim3 bgrid((unsigned)(cdiv(d.Nf, 32) * cdiv(d.Nz, 8)), 4 * q_count);
-    if (!rc) {
-      prep_b<<<bgrid, 256, smb, ctx->stream>>>(P, ctx->s.chi_ph, ctx->s.chi_pp, ctx->s.bse_B, q_begin, d.Nz, d.Nf,
-                                               d.Nl);
-      rc = after_launch(ctx, "k_bse_prep_b");
-    }
-  }
+  int rc = prep_chunk(ctx, P, q_begin, q_count);
   phase_end(ctx, TUPS_PHASE_BSE_PREP);
   if (rc) return rc;
   if (slices > 0) {
