@@ -363,13 +363,29 @@ extern "C" int tups_iteration(tups_ctx* ctx, int ite, tups_conv_info* info) {
 // SigmaOld = Sigma and the vertex update.  The output block only moves mu
 // and does not touch the vertices, so it follows the update on the host;
 // the update does not change F, so max|F_r| is taken in the update's own
-// pass over F.
+// pass over F.  The SDE reads Phi (the BSE's output), the Green's function
+// and the bubbles and writes only its own arrays and Sigma, none of which
+// Phi(R) or the crossing read or write, so with a side stream it runs there
+// beside them (its small kernels fill SMs the crossing's tail leaves idle)
+// and joins before the conv kernels.
 static int iteration_device(tups_ctx* ctx, int slices, bool do_sde) {
   TRY(green_async(ctx, 0));
   TRY(bse_async(ctx, slices));
+  const bool fork = do_sde && ctx->side_stream && ctx->fork_ev && ctx->join_ev;
+  if (fork) {
+    TRY(tups::cuda_check(ctx, cudaEventRecord(ctx->fork_ev, ctx->stream), "fork"));
+    TRY(tups::cuda_check(ctx, cudaStreamWaitEvent(ctx->side_stream, ctx->fork_ev, 0), "fork"));
+    cudaStream_t main = ctx->stream;
+    ctx->stream = ctx->side_stream;
+    const int rc = sde_async(ctx);
+    ctx->stream = main;
+    TRY(rc);
+    TRY(tups::cuda_check(ctx, cudaEventRecord(ctx->join_ev, ctx->side_stream), "join"));
+  }
   TRY(tups::launch_phir(ctx));
   TRY(tups::launch_pae(ctx));
-  if (do_sde) TRY(sde_async(ctx));
+  if (do_sde && !fork) TRY(sde_async(ctx));
+  if (fork) TRY(tups::cuda_check(ctx, cudaStreamWaitEvent(ctx->stream, ctx->join_ev, 0), "join"));
   TRY(tups::launch_conv_sigma(ctx));
   TRY(copy_sigma_old(ctx));
   return tups::launch_vertex_update_fmax(ctx);
@@ -383,6 +399,11 @@ static int iteration_graph(tups_ctx* ctx, int ite, tups_conv_info* info) {
   const bool do_sde = !ctx->p.oneshot || ite == ctx->p.ite_max - 1;
   const int key = sl * 2 + (do_sde ? 1 : 0);
   if (!ctx->graph_exec[key]) {
+    if (!ctx->side_stream) {
+      TRY(tups::cuda_check(ctx, cudaStreamCreateWithFlags(&ctx->side_stream, cudaStreamNonBlocking), "side stream"));
+      TRY(tups::cuda_check(ctx, cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming), "fork event"));
+      TRY(tups::cuda_check(ctx, cudaEventCreateWithFlags(&ctx->join_ev, cudaEventDisableTiming), "join event"));
+    }
     const long long l0 = ctx->launches;
     TRY(tups::cuda_check(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed), "begin capture"));
     ctx->capturing = true;

@@ -762,6 +762,11 @@ static void free_all(tups_ctx* ctx) {
       g = nullptr;
     }
   tups::destroy_events(ctx);
+  if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
+  if (ctx->join_ev) cudaEventDestroy(ctx->join_ev);
+  if (ctx->side_stream) cudaStreamDestroy(ctx->side_stream);
+  ctx->fork_ev = ctx->join_ev = nullptr;
+  ctx->side_stream = nullptr;
   for (void* p : ctx->allocations) cudaFree(p);
   ctx->allocations.clear();
   if (ctx->stream) cudaStreamDestroy(ctx->stream);

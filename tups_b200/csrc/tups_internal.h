@@ -154,6 +154,10 @@ struct tups_ctx {
   int pae_products = 3;        // real DMMA products per complex one in the crossing GEMM (3 or 4)
   long long tile_tunings = 0;
   cudaGraphExec_t graph_exec[18] = {};
+  // second stream of a captured iteration: the SDE runs on it beside
+  // Phi(R) and the crossing (created before the first capture)
+  cudaStream_t side_stream = nullptr;
+  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
   long long graph_launches[18] = {};
   double tune_graph_ms[9] = {-1, -1, -1, -1, -1, -1, -1, -1, -1};
   double ck_scal[16] = {};
