@@ -26,8 +26,10 @@
 // whole parquet equation is ONE complex GEMM
 //     C^T[(target, element), (l1,l2)] = X^T[(target, element), (family,l3,l4,R)] M^T
 // run on the FP64 tensor cores (mma.sync m16n8k8), with X gathered from
-// Phi(R) on load and F = Phi + Lambda*Nc + C/Nx written once in the epilogue:
-// no atomics, deterministic.
+// Phi(R) on load and F = Phi + Lambda*Nc + C/Nx: a base pass writes
+// Phi + Lambda*Nc, and each family pass adds C/Nx to the elements it reaches
+// by reductions in L2, each element at most once per pass, so the result
+// does not depend on the order of the CTAs (deterministic).
 #include <string>
 
 #include "tups_device.cuh"
@@ -423,9 +425,12 @@ __global__ void __launch_bounds__(32 * RW * WN, RW * WN == 8 ? (TN <= 2 ? PAE_MI
       const int rw = x >= 2 ? rw1 : rw0;
       const long long c = ecol[(wc * TN + j) * 8 + 2 * tig + (x & 1)];
       if (rw < 0 || c < 0) continue;
+      // a reduction in L2 (no value returned, so no wait for the old F);
+      // each element is in a family's list once, so no two CTAs of a launch
+      // add to the same entry
       cplx* f = Ft + c + rw;
-      const cplx v = *f;
-      *f = cmk(v.x + inv_nx * cre[j][x], v.y + inv_nx * cim[j][x]);
+      atomicAdd(&f->x, __dmul_rn(inv_nx, cre[j][x]));
+      atomicAdd(&f->y, __dmul_rn(inv_nx, cim[j][x]));
     }
 }
 
