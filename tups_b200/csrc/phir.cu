@@ -58,12 +58,29 @@ __host__ __device__ constexpr int phir_max_threads(int opt, int nr) {
 // stage Phi[(a, ni0 + t), (b, nj)] (t < PH_TI, all a, b < Nl) of one slot
 // into dst[(a + Nl b) PH_TI + t]; src points at element (0, nj) of the
 // slot; entries with ni >= Nf are zero-filled
-__device__ __forceinline__ void ph_stage(cplx* dst, const cplx* src, int n, int Nl, int Nf, int Nz, int ni0) {
-  for (int x = threadIdx.x; x < n; x += blockDim.x) {
-    const int t = x % PH_TI, ab = x / PH_TI;
-    const int a = ab % Nl, b = ab / Nl, ni = ni0 + t;
-    const bool ok = ni < Nf;
-    ph_cp_async16(dst + x, ok ? src + (a * Nf + ni) + (size_t)Nz * Nf * b : src, ok);
+// (the same entries for every slot: the source offsets are computed once
+// per thread, ph_offsets, and reused for every momentum; -1 = zero fill,
+// -2 = no entry; a thread owns at most NC entries, NC blockDim >= n)
+template <int NC>
+__device__ __forceinline__ void ph_offsets(int* off, int n, int Nl, int Nf, int Nz, int ni0) {
+#pragma unroll
+  for (int u = 0; u < NC; u++) {
+    const int x = threadIdx.x + u * blockDim.x;
+    off[u] = -2;
+    if (x < n) {
+      const int t = x % PH_TI, ab = x / PH_TI;
+      const int a = ab % Nl, b = ab / Nl, ni = ni0 + t;
+      off[u] = ni < Nf ? (a * Nf + ni) + Nz * Nf * b : -1;
+    }
+  }
+}
+template <int NC>
+__device__ __forceinline__ void ph_stage(cplx* dst, const cplx* src, const int* off) {
+#pragma unroll
+  for (int u = 0; u < NC; u++) {
+    if (off[u] == -2) continue;
+    const bool ok = off[u] >= 0;
+    ph_cp_async16(dst + threadIdx.x + u * blockDim.x, ok ? src + off[u] : src, ok);
   }
 }
 
@@ -159,13 +176,15 @@ __global__ void __launch_bounds__(phir_max_threads(OPT, NR)) k_phir(PhirPtrs P, 
   const cplx* G = r == 0 ? P.G[0] : r == 1 ? P.G[1] : r == 2 ? P.G[2] : P.G[3];
   const int stage_elems = nl2 * PH_TI;
   const cplx* Gw = G + (size_t)Nz * nj;  // element (0, (0, nj)); column (b, nj) is Nz Nf b further
+  // stage_elems = Nl^2 PH_TI <= OPT blockDim: at most OPT copies per thread
+  int soff[OPT];
+  ph_offsets<OPT>(soff, stage_elems, Nl, Nf, Nz, ni0);
   // three buffers, momenta staged two ahead: the barrier at the top of an
   // iteration both publishes this momentum's stage and ends every read of
   // the buffer the next copy overwrites, so one barrier per momentum
 #pragma unroll
   for (int qq = 0; qq < PH_STAGES - 1; qq++) {
-    if (qq < nq) ph_stage(sPhi + (size_t)qq * stage_elems, Gw + n2 * (size_t)(sQ[qq] * nh + w - slot0), stage_elems,
-                          Nl, Nf, Nz, ni0);
+    if (qq < nq) ph_stage<OPT>(sPhi + (size_t)qq * stage_elems, Gw + n2 * (size_t)(sQ[qq] * nh + w - slot0), soff);
     asm volatile("cp.async.commit_group;\n" ::);
   }
   for (int qi = 0; qi < nq; qi++) {
@@ -174,8 +193,8 @@ __global__ void __launch_bounds__(phir_max_threads(OPT, NR)) k_phir(PhirPtrs P, 
     {
       const int qn = qi + PH_STAGES - 1;
       if (qn < nq)
-        ph_stage(sPhi + (size_t)(qn % PH_STAGES) * stage_elems, Gw + n2 * (size_t)(sQ[qn] * nh + w - slot0),
-                 stage_elems, Nl, Nf, Nz, ni0);
+        ph_stage<OPT>(sPhi + (size_t)(qn % PH_STAGES) * stage_elems, Gw + n2 * (size_t)(sQ[qn] * nh + w - slot0),
+                      soff);
       asm volatile("cp.async.commit_group;\n" ::);
     }
     const cplx* S = sPhi + (size_t)(qi % PH_STAGES) * stage_elems;
