@@ -539,8 +539,9 @@ static const PaeCand kPaeWide[] = {
 // crossing-products setting.  "g3p" candidates rewrite each landed X stage
 // as per-target operands (PRE); "_s3" ones run a three-stage pipeline.
 // Index 0 is the tuner's pick on a B200: at 8x8 / Nl = 5 64 flat columns
-// (1.35 ms against 1.37 for the PRE form on 32), at 16x16 / Nl = 9 the PRE
-// form on 64 columns (327 ms against 333 on 48 and 345 without PRE).
+// (1.24 ms against 1.25 for the PRE form on 64 and 1.31-1.37 for the rest),
+// at 16x16 / Nl = 9 the PRE form on 64 columns (316 ms against 318 on 48
+// and 338 without PRE).
 static const PaeCand kPaeNl5G3[] = {
     {"g3_flat_bn64_tn4", run_pae<4, 2, 4, 2, 0, true>, 64},
     {"g3p_flat_bn32_tn2", run_pae<2, 2, 4, 2, 0, true, true>, 32},
