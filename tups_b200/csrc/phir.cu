@@ -97,6 +97,8 @@ __global__ void __launch_bounds__(phir_max_threads(OPT, NR)) k_phir(PhirPtrs P, 
   int* sSym = reinterpret_cast<int*>(sE + (size_t)npairs * NR);  // [npairs] symmetry of pair p
   int* sBeg = sSym + npairs;                               // [NIBZ + 1] first pair of Q
   int* sQ = sBeg + NIBZ + 1;                               // [NIBZ] momenta of this context at w
+  // [NS][blockDim]: this thread's permuted offset per symmetry, sign in bit 31
+  unsigned* sOff = reinterpret_cast<unsigned*>(sQ + NIBZ);
   __shared__ int sNq;
 
   const int ntile = (Nf + PH_TI - 1) / PH_TI;
@@ -154,15 +156,14 @@ __global__ void __launch_bounds__(phir_max_threads(OPT, NR)) k_phir(PhirPtrs P, 
   // this thread's outputs: pair p, permuted-pair offsets and signs per symmetry
   const int p = threadIdx.x / SUB, c = threadIdx.x % SUB;
   const bool active = p < nl2;
-  unsigned offpk[NS / 2] = {0u, 0u, 0u, 0u};
-  unsigned negmask = 0u;
+  // (each thread reads back only its own entries: no barrier)
   if (active) {
     const int li = p % Nl, lj = p / Nl;
 #pragma unroll
     for (int sy = 0; sy < NS; sy++) {
       const unsigned o = (unsigned)((lsym[sy + NS * li] + Nl * lsym[sy + NS * lj]) * PH_TI + c);
-      offpk[sy >> 1] |= o << (16 * (sy & 1));
-      if (lfac[sy + NS * li] * lfac[sy + NS * lj] < 0.0) negmask |= 1u << sy;
+      const unsigned neg = lfac[sy + NS * li] * lfac[sy + NS * lj] < 0.0 ? 1u : 0u;
+      sOff[sy * blockDim.x + threadIdx.x] = o | (neg << 31);
     }
   }
   cplx acc[OPT][NR];
@@ -206,9 +207,9 @@ __global__ void __launch_bounds__(phir_max_threads(OPT, NR)) k_phir(PhirPtrs P, 
 #pragma unroll
       for (int R = 0; R < NR; R++) e[R] = sE[pp * NR + R];
       if (active) {
-        const unsigned wpk = sy < 4 ? (sy < 2 ? offpk[0] : offpk[1]) : (sy < 6 ? offpk[2] : offpk[3]);
-        const unsigned off = (sy & 1) ? wpk >> 16 : wpk & 0xffffu;
-        const unsigned neg = negmask >> sy & 1u;
+        const unsigned word = sOff[sy * blockDim.x + threadIdx.x];
+        const unsigned off = word & 0x7fffffffu;
+        const unsigned neg = word >> 31;
 #pragma unroll
         for (int k = 0; k < OPT; k++) {
           cplx v = S[off + SUB * k];
@@ -325,7 +326,7 @@ static int phir_run(tups_ctx* ctx, const PhirPtrs& P, int cand) {
   const int threads = phir_threads(ctx, cand);
   if (!phir_fits(ctx, cand)) return set_error(ctx, TUPS_ERR_BADDIM, "k_phir: too many form-factor pairs for one CTA");
   const size_t sm = (size_t)PH_STAGES * nl2 * PH_TI * sizeof(cplx) + (size_t)npairs * d.NR * sizeof(cplx) +
-                    ((size_t)npairs + 2 * d.NIBZ + 1) * sizeof(int);
+                    ((size_t)npairs + 2 * d.NIBZ + 1) * sizeof(int) + (size_t)NS * threads * sizeof(unsigned);
   if (sm > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return cuda_check(ctx, e, "k_phir smem attribute");
