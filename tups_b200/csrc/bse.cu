@@ -4,7 +4,8 @@
 //   Phi_r = c_r f [ (a Gamma chi) F + F (a chi Gamma) ] + (1-f)(F - Gamma),
 // a = 1/(beta Nx Ny), c_d = c_m = 1/2 (chi_ph), c_s = -1/4, c_t = +1/4 (chi_pp).
 // chi is block-diagonal in nu (one Nl x Nl block per nu), so Gamma chi and
-// chi Gamma cost Nz^2 Nl each (k_bse_prep).  The remaining work is ONE complex
+// chi Gamma cost Nz^2 Nl each (k_bse_prep + k_bse_prep_b, or the two in one
+// launch, k_bse_prep_ab: a tuner choice).  The remaining work is ONE complex
 // GEMM with K = 2 Nz,  [Gamma chi | F] x [F ; chi Gamma],  run on the FP64
 // tensor cores (mma.sync m16n8k8 f64, k_bse_gemm) with the scale and the
 // damping term fused into the epilogue; Phi_r overwrites Gamma_r in place.
